@@ -1,0 +1,141 @@
+/* RapidBoW-B200: C ABI of the B200-native vocabulary-tree hot path.
+ *
+ * Every entry point returns an rbw_status (0 = RBW_OK) and never throws; the message of the
+ * last failure on the calling thread is available from rbw_last_error().  Handles are opaque.
+ * `stream` arguments are cudaStream_t values passed as void* (NULL = legacy default stream).
+ * Device buffers are plain device (or managed) pointers; descriptor rows are 128 uint8 bytes
+ * and must start on a 16-byte boundary, as the reference requires (vocTreeLookUp.cu:42,71).
+ *
+ * Each declaration names the reference interface it replaces (file:line in lowsfer/RapidBoW).
+ */
+#ifndef RAPIDBOW_B200_H
+#define RAPIDBOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RBW_API __attribute__((visibility("default")))
+#else
+#define RBW_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    RBW_OK = 0,
+    RBW_ERR_INVALID_ARG = 1,   /* std::runtime_error on bad input in the reference */
+    RBW_ERR_UNSUPPORTED = 2,   /* the reference prints and returns nullptr (RapidBoW.cpp:37-40) */
+    RBW_ERR_OUT_OF_MEMORY = 3,
+    RBW_ERR_CUDA = 4,          /* cudaCheck failures */
+    RBW_ERR_TIMEOUT = 5,       /* a device-side bounded wait gave up */
+    RBW_ERR_INVALID_BLOB = 6,  /* "invalid blob" (Vocabulary.cpp:128-144) */
+    RBW_ERR_DUPLICATE = 7,     /* "Duplicate document index" (DataBase.cpp:41-43) */
+    RBW_ERR_INTERNAL = 8
+} rbw_status;
+
+/* Values match rbow::DataType / rbow::DistanceType (RapidBoW.h:32-48). */
+enum { RBW_DATA_BINARY = 0, RBW_DATA_UINT8 = 1 };
+enum { RBW_DIST_HAMMING = 0, RBW_DIST_L1 = 1, RBW_DIST_L2 = 2 };
+typedef struct {
+    int32_t data_type;
+    int32_t distance_type;
+    uint64_t nb_dims;
+} rbw_desc_attr;
+
+/* Initial-center choice for the k-means of every node. */
+enum {
+    RBW_INIT_REFERENCE = 0, /* the reference's random distinct picks (kmeans.cpp:260-315), default seed */
+    RBW_INIT_KMEANSPP = 1,  /* seeded k-means++ over <= 256 sampled members per node */
+    RBW_INIT_INJECTED = 2   /* caller-provided descriptor indices per node */
+};
+
+/* Build flags.  The reference rounds centers with its --use_fast_math division
+ * (kmeans.cu:367); RBW_BUILD_IEEE_DIVISION uses the correctly rounded quotient instead. */
+enum { RBW_BUILD_IEEE_DIVISION = 1 };
+
+typedef struct {
+    uint32_t max_iterations;       /* Lloyd cap; reference: 1000 (kmeans.h:118) */
+    uint32_t check_interval;       /* host convergence poll; reference: 4 (kmeans.h:115) */
+    uint32_t init_mode;            /* RBW_INIT_* */
+    uint32_t flags;                /* RBW_BUILD_* bits */
+    uint64_t seed;                 /* RBW_INIT_KMEANSPP */
+    const uint32_t* injected_init; /* RBW_INIT_INJECTED: host [levelBeg(L)][B], UINT32_MAX = invalid */
+} rbw_build_options;
+
+typedef struct rbw_vocabulary rbw_vocabulary;
+
+/* Lookup algorithms. */
+enum {
+    RBW_LOOKUP_AUTO = 0,       /* fastest exact path */
+    RBW_LOOKUP_TENSOR_U8 = 1,  /* tcgen05 uint8 tensor-core descent with device regroup */
+    RBW_LOOKUP_SIMT_F32 = 2    /* plain FP32 SIMT descent (comparison baseline) */
+};
+
+RBW_API const char* rbw_last_error(void);
+RBW_API const char* rbw_version(void);
+RBW_API void rbw_build_options_default(rbw_build_options* opts);
+
+/* Replaces rbow::impl::buildVocabularyImpl (RapidBoW.h:75-79, RapidBoW.cpp:26-41) and
+ * buildSiftVocabulary (Vocabulary.cpp:32-121).  Synchronous on `stream`.  opts may be NULL
+ * (reference defaults).  SIFT attributes only (uint8, L2, 128 dims); branch factor 2..16. */
+RBW_API int rbw_voc_build(rbw_desc_attr attr, uint32_t branch_factor, const void* dev_desc, uint32_t nb_desc,
+                          uint32_t nb_doc, uint32_t nb_levels, const rbw_build_options* opts, void* stream,
+                          rbw_vocabulary** out);
+
+/* Builds a vocabulary from host arrays: centers [levelBeg(L)][B][128] uint8, masks
+ * [levelBeg(L)], weights [levelBeg(L)][B] (the fields of Vocabulary, Vocabulary.h:44-51). */
+RBW_API int rbw_voc_from_host(uint32_t branch_factor, uint32_t nb_levels, const uint8_t* centers,
+                              const uint32_t* masks, const float* weights, rbw_vocabulary** out);
+
+/* Replaces IVocabulary::lookUp (RapidBoW.h:66-68, Vocabulary.h:59-63): leaf index per descriptor
+ * in [0, B^L), asynchronous on `stream`, device buffers. */
+RBW_API int rbw_voc_lookup(const rbw_vocabulary* voc, const void* dev_desc, uint32_t nb_desc, uint32_t* dev_leaf,
+                           void* stream);
+
+/* lookUp with an explicit algorithm; reports the number of kernels it launched. */
+RBW_API int rbw_voc_lookup_ex(const rbw_vocabulary* voc, const void* dev_desc, uint64_t nb_desc, uint32_t* dev_leaf,
+                              int32_t algo, void* stream, uint32_t* kernels_launched);
+
+/* lookUp from host memory to host memory: copies descriptors in, looks them up and copies the
+ * leaf indices back, pipelined in chunks over two streams; returns when results are on the
+ * host.  Host buffers should be pinned for full PCIe bandwidth. */
+RBW_API int rbw_voc_lookup_host(const rbw_vocabulary* voc, const void* host_desc, uint64_t nb_desc,
+                                uint32_t* host_leaf, int32_t algo, uint32_t* kernels_launched);
+
+/* Replaces IVocabulary::serialize (RapidBoW.h:69, Vocabulary.cpp:175-198).  With buf == NULL
+ * only *size is set.  For B = 16 the bytes are the reference's blob format. */
+RBW_API int rbw_voc_serialize(const rbw_vocabulary* voc, uint8_t* buf, uint64_t capacity, uint64_t* size);
+
+/* Replaces rbow::deserializeVocabulary (RapidBoW.h:90, Vocabulary.cpp:126-157). */
+RBW_API int rbw_voc_deserialize(const uint8_t* blob, uint64_t size, rbw_vocabulary** out);
+
+/* getDescriptorAttributes / getBranchFactor / getNbLevels (RapidBoW.h:63-65). */
+RBW_API int rbw_voc_info(const rbw_vocabulary* voc, rbw_desc_attr* attr, uint32_t* branch_factor, uint32_t* nb_levels,
+                         uint64_t* nb_nodes);
+
+/* Replaces IVocabularyInternal::getLevelWeights (RapidBoWInternal.h:26-31): host pointer to
+ * float[levelSize(level)][B], valid for the lifetime of the vocabulary. */
+RBW_API int rbw_voc_level_weights(const rbw_vocabulary* voc, uint32_t level, const float** host_weights);
+
+/* Copies the tree out: centers [levelBeg(L)][B][128], masks [levelBeg(L)], weights
+ * [levelBeg(L)][B] (any pointer may be NULL).  Test and tooling helper. */
+RBW_API int rbw_voc_get_tree(const rbw_vocabulary* voc, uint8_t* host_centers, uint32_t* host_masks,
+                             float* host_weights);
+
+/* Device scratch bytes rbw_voc_lookup needs for nb_desc descriptors. */
+RBW_API int rbw_voc_lookup_scratch_bytes(const rbw_vocabulary* voc, uint64_t nb_desc, uint64_t* bytes);
+
+/* Reads and clears the device-side error record (set by a bounded wait that timed out).
+ * Synchronizes the device. */
+RBW_API int rbw_voc_device_errors(const rbw_vocabulary* voc, uint32_t* code, uint32_t* where);
+
+/* Replaces IVocabulary::~IVocabulary (RapidBoW.cpp:24). */
+RBW_API void rbw_voc_destroy(rbw_vocabulary* voc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,755 @@
+// Vocabulary-tree descent kernels (reference semantics: vocTreeLookUp.cu:82-155 -- exact
+// squared L2 over 16 centers per node, lowest branch index on ties, idx = idx*B + b).
+//
+// Two implementations behind launchLookup():
+//   * lookupPassTc  : tcgen05 kind::i8 (u8 x u8 -> s32, exact) over level pairs.  A pass takes
+//                     the descriptors grouped by their node at level 2p, stages 128-row tiles with
+//                     TMA (tiled load for the first pass, tile::gather4 through a permutation
+//                     afterwards), runs one MMA against the node's 16 centers (level 2p) and one
+//                     against all of its children's centers (level 2p+1, N = 16*B), and picks the
+//                     argmin of |c|^2 - 2 x.c from tensor memory.  Between passes a device
+//                     counting sort (histogram fused into the pass epilogue, scan, scatter)
+//                     groups the descriptors by their node at level 2p+2.
+//   * lookupSimtF32 : plain FP32 SIMT kernel (16 threads per descriptor, one center each),
+//                     the comparison baseline.  Exact for uint8 data (all sums < 2^24).
+#include "lookup.cuh"
+
+#include <algorithm>
+#include <mutex>
+
+namespace rbw {
+namespace {
+
+struct TileInfo {
+    uint32_t group;
+    uint32_t start;
+    uint32_t count;
+    uint32_t pad;
+};
+
+constexpr uint32_t kStages = 4;
+constexpr uint32_t kTileRows = 128;
+constexpr uint32_t kTileBytes = kTileRows * kDims;    // 16 KB
+constexpr uint32_t kNodeBytes = kMaxBranch * kDims;   // 2 KB: one node's 16 centers
+constexpr uint32_t kBBlockBytes = kNodeBytes * 17;    // node + up to 16 children
+constexpr uint32_t kTcThreads = 192;                  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr uint32_t kEpiThreads = 128;
+constexpr uint32_t kSmemHistMax = 4096;
+constexpr uint32_t kTmemCols = 512;                   // two accumulator buffers of 256 columns
+
+struct TcSmem {
+    uint8_t a[kStages][kTileBytes];
+    uint8_t b[2][kBBlockBytes];
+    uint64_t aFull[kStages];
+    uint64_t aEmpty[kStages];
+    uint64_t bFull[2];
+    uint64_t bEmpty[2];
+    uint64_t accA[2];
+    uint64_t accAFree[2];
+    uint64_t accB[2];
+    uint64_t accBFree[2];
+    uint64_t mmaDone;
+    uint32_t tmemBase;
+    uint32_t abortFlag;
+    uint32_t hist[kSmemHistMax];
+};
+constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 1024;
+
+struct PassParams {
+    const uint8_t* centersSw;
+    const int32_t* cnorm;
+    uint32_t B;
+    uint32_t twoLevels;
+    uint64_t lbA;            // levelBeg of the level the groups live on (2p)
+    uint64_t lbB;            // levelBeg(2p + 1)
+    uint64_t nRows;
+    const uint32_t* perm;    // nullptr for the first pass (rows in input order)
+    const TileInfo* tiles;   // nullptr for the first pass
+    const uint32_t* nTilesDev;
+    uint32_t* out;           // final pass: leaf index per descriptor
+    uint32_t* nodeNext;      // other passes: in-level node index at level 2p + 2
+    uint32_t* binCount;      // other passes: histogram of nodeNext
+    uint32_t nbBins;
+    uint32_t isFinal;
+    DeviceErrors* err;
+};
+
+__device__ __forceinline__ TileInfo getTile(const PassParams& p, uint32_t t)
+{
+    if (p.tiles == nullptr) {
+        const uint64_t s = uint64_t(t) * kTileRows;
+        const uint64_t c = p.nRows - s < kTileRows ? p.nRows - s : kTileRows;
+        return TileInfo{0u, static_cast<uint32_t>(s), static_cast<uint32_t>(c), 0u};
+    }
+    return p.tiles[t];
+}
+
+// Waits until the tcgen05.ld results are in registers; the operands tie the 16 registers to
+// the wait so no use of them is scheduled before it.
+__device__ __forceinline__ void tmemWaitTie(uint32_t (&r)[16])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                   "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]),
+                   "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
+}
+__device__ __forceinline__ void tieRegs(uint32_t (&r)[16])
+{
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                   "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]),
+                   "+r"(r[14]), "+r"(r[15]));
+}
+
+// argmin_b (|c_b|^2 - 2 x.c_b), lowest b on ties (vocTreeLookUp.cu:108-125).
+__device__ __forceinline__ uint32_t argminScores(const uint32_t (&dot)[16], const int32_t* cnormNode)
+{
+    const int4* cn4 = reinterpret_cast<const int4*>(cnormNode);
+    int32_t cn[16];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int4 v = __ldg(cn4 + i);
+        cn[4 * i] = v.x;
+        cn[4 * i + 1] = v.y;
+        cn[4 * i + 2] = v.z;
+        cn[4 * i + 3] = v.w;
+    }
+    int32_t best = cn[0] - 2 * static_cast<int32_t>(dot[0]);
+    uint32_t bi = 0;
+#pragma unroll
+    for (uint32_t b = 1; b < 16; b++) {
+        const int32_t s = cn[b] - 2 * static_cast<int32_t>(dot[b]);
+        if (s < best) {
+            best = s;
+            bi = b;
+        }
+    }
+    return bi;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    lookupPassTc(const __grid_constant__ CUtensorMap tmapTile, const __grid_constant__ CUtensorMap tmapRow,
+                 const PassParams p)
+{
+    extern __shared__ uint8_t smemRaw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+    const uint32_t warp = threadIdx.x / 32;
+    const uint32_t lane = threadIdx.x % 32;
+    const uint32_t T = p.tiles == nullptr ? static_cast<uint32_t>((p.nRows + kTileRows - 1) / kTileRows)
+                                          : *p.nTilesDev;
+    const uint32_t t0 = static_cast<uint32_t>(uint64_t(T) * blockIdx.x / gridDim.x);
+    const uint32_t t1 = static_cast<uint32_t>(uint64_t(T) * (blockIdx.x + 1) / gridDim.x);
+    const uint32_t nT = t1 - t0;
+    const bool smemHist = !p.isFinal && p.nbBins <= kSmemHistMax;
+    const bool two = p.twoLevels != 0;
+    volatile uint32_t* abortFlag = &S.abortFlag;
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < kStages; s++) {
+            mbarInit(&S.aFull[s], 1);
+            mbarInit(&S.aEmpty[s], 1);
+        }
+        for (uint32_t j = 0; j < 2; j++) {
+            mbarInit(&S.bFull[j], 1);
+            mbarInit(&S.bEmpty[j], 1);
+            mbarInit(&S.accA[j], 1);
+            mbarInit(&S.accAFree[j], kEpiThreads);
+            mbarInit(&S.accB[j], 1);
+            mbarInit(&S.accBFree[j], kEpiThreads);
+        }
+        mbarInit(&S.mmaDone, 1);
+        S.abortFlag = 0;
+        fenceMbarInit();
+    }
+    if (smemHist) {
+        for (uint32_t i = threadIdx.x; i < p.nbBins; i += blockDim.x) S.hist[i] = 0;
+    }
+    if (warp == 0) {
+        tmemAlloc(&S.tmemBase, kTmemCols);
+        tmemRelinquish();
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tmem = S.tmemBase;
+
+    if (nT > 0 && warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, slotUses[2] = {0, 0};
+        for (uint32_t i = 0; i < nT; i++) {
+            const TileInfo ti = getTile(p, t0 + i);
+            bool ok = true;
+            if (ti.group != prevGroup) {
+                slot ^= 1u;
+                const uint32_t k = slotUses[slot]++;
+                if (lane == 0) {
+                    ok = mbarWait(&S.bEmpty[slot], (k & 1u) ^ 1u, abortFlag, p.err, 10);
+                    if (ok) {
+                        const uint32_t bytes = kNodeBytes * (two ? 1u + p.B : 1u);
+                        mbarArriveExpectTx(&S.bFull[slot], bytes);
+                        bulkLoad(S.b[slot], p.centersSw + (p.lbA + ti.group) * kNodeBytes, kNodeBytes, &S.bFull[slot]);
+                        if (two) {
+                            bulkLoad(S.b[slot] + kNodeBytes,
+                                     p.centersSw + (p.lbB + uint64_t(ti.group) * p.B) * kNodeBytes, kNodeBytes * p.B,
+                                     &S.bFull[slot]);
+                        }
+                    }
+                }
+                ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+                if (!ok) break;
+                prevGroup = ti.group;
+            }
+            const uint32_t s = i % kStages;
+            const uint32_t ph = (i / kStages) & 1u;
+            if (lane == 0) {
+                ok = mbarWait(&S.aEmpty[s], ph ^ 1u, abortFlag, p.err, 11);
+                if (ok) mbarArriveExpectTx(&S.aFull[s], kTileBytes);
+            }
+            ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+            if (!ok) break;
+            if (p.perm == nullptr) {
+                if (lane == 0) tmaLoad2d(S.a[s], &tmapTile, 0, static_cast<int32_t>(ti.start), &S.aFull[s]);
+            } else {
+                // lane q gathers rows 4q..4q+3 of the tile (rows past the group end repeat row 0).
+                int32_t r[4];
+#pragma unroll
+                for (uint32_t j = 0; j < 4; j++) {
+                    const uint32_t rr = 4 * lane + j;
+                    r[j] = static_cast<int32_t>(__ldg(p.perm + ti.start + (rr < ti.count ? rr : 0u)));
+                }
+                tmaGather4(S.a[s] + lane * 512u, &tmapRow, 0, r[0], r[1], r[2], r[3], &S.aFull[s]);
+            }
+            __syncwarp();
+        }
+        // Drain: every stage this warp armed must have landed before the CTA can exit.
+        if (lane == 0) {
+            const uint32_t armed = nT < kStages ? nT : kStages;
+            for (uint32_t s = 0; s < armed; s++) {
+                const uint32_t last = ((nT - 1 - s) / kStages) * kStages + s; // last i with i % kStages == s
+                if (last < nT) mbarWait(&S.aFull[s], (last / kStages) & 1u, abortFlag, nullptr, 12);
+            }
+        }
+        __syncwarp();
+    } else if (nT > 0 && warp == 1) {
+        // ------------------------------------------------------------ MMA issuer (one thread)
+        if (lane == 0) {
+            const uint32_t idescA = idescU8(16);
+            const uint32_t idescB = idescU8(16 * p.B);
+            uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, slotUses[2] = {0, 0};
+            uint32_t slotOf[2] = {0, 0};  // B slot of tile t, ring indexed by t & 1
+            bool ok = true;
+            auto releaseIfLast = [&](uint32_t t) {
+                const uint32_t g = getTile(p, t0 + t).group;
+                const bool last = (t + 1 >= nT) || getTile(p, t0 + t + 1).group != g;
+                if (last) mmaCommit(&S.bEmpty[slotOf[t & 1u]]);
+            };
+            auto issueA = [&](uint32_t t) -> bool {
+                const TileInfo ti = getTile(p, t0 + t);
+                if (ti.group != prevGroup) {
+                    slot ^= 1u;
+                    const uint32_t k = slotUses[slot]++;
+                    if (!mbarWait(&S.bFull[slot], k & 1u, abortFlag, p.err, 20)) return false;
+                    prevGroup = ti.group;
+                }
+                slotOf[t & 1u] = slot;
+                const uint32_t s = t % kStages;
+                if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21)) return false;
+                const uint32_t buf = t & 1u;
+                if (t >= 2) {
+                    uint64_t* freeBar = two ? &S.accBFree[buf] : &S.accAFree[buf];
+                    if (!mbarWait(freeBar, ((t >> 1) - 1u) & 1u, abortFlag, p.err, 22)) return false;
+                }
+                tcFenceAfter();
+                const uint32_t aBase = smemAddr(S.a[s]);
+                const uint32_t bBase = smemAddr(S.b[slot]);
+#pragma unroll
+                for (uint32_t k = 0; k < 4; k++) {
+                    mmaU8(tmem + buf * 256u, smemDescSw128(aBase + 32u * k), smemDescSw128(bBase + 32u * k), idescA,
+                          k > 0 ? 1u : 0u);
+                }
+                mmaCommit(&S.accA[buf]);
+                if (!two) {
+                    mmaCommit(&S.aEmpty[s]);
+                    releaseIfLast(t);
+                }
+                return true;
+            };
+            auto issueB = [&](uint32_t t) -> bool {
+                const uint32_t buf = t & 1u;
+                const uint32_t s = t % kStages;
+                if (!mbarWait(&S.accAFree[buf], (t >> 1) & 1u, abortFlag, p.err, 23)) return false;
+                tcFenceAfter();
+                const uint32_t aBase = smemAddr(S.a[s]);
+                const uint32_t bBase = smemAddr(S.b[slotOf[t & 1u]]) + kNodeBytes;
+#pragma unroll
+                for (uint32_t k = 0; k < 4; k++) {
+                    mmaU8(tmem + buf * 256u, smemDescSw128(aBase + 32u * k), smemDescSw128(bBase + 32u * k), idescB,
+                          k > 0 ? 1u : 0u);
+                }
+                mmaCommit(&S.accB[buf]);
+                mmaCommit(&S.aEmpty[s]);
+                releaseIfLast(t);
+                return true;
+            };
+            if (two) {
+                // Tensor-core order a0 a1 b0 | b1 a2 | b2 a3 | ... : the next tile's level-2p MMA
+                // runs while the epilogue reads the current tile's children block.
+                ok = issueA(0);
+                if (ok && nT > 1) ok = issueA(1);
+                if (ok) ok = issueB(0);
+                for (uint32_t t = 1; ok && t < nT; t++) {
+                    ok = issueB(t);
+                    if (ok && t + 1 < nT) ok = issueA(t + 1);
+                }
+            } else {
+                for (uint32_t t = 0; ok && t < nT; t++) ok = issueA(t);
+            }
+            mmaCommit(&S.mmaDone);
+            mbarWait(&S.mmaDone, 0, abortFlag, nullptr, 24);
+        }
+        __syncwarp();
+    } else if (nT > 0 && warp >= 2) {
+        // ------------------------------------------------------------ epilogue (128 threads = 128 rows)
+        const uint32_t q = warp & 3u;
+        const uint32_t row = q * 32u + lane;
+        const uint32_t tRow = tmem + ((q * 32u) << 16);
+        uint32_t bstar0 = 0, bstar1 = 0;
+        auto finalize = [&](const TileInfo& ti, uint32_t node) {
+            if (row < ti.count) {
+                const uint32_t orig = p.perm == nullptr ? ti.start + row : __ldg(p.perm + ti.start + row);
+                if (p.isFinal) {
+                    p.out[orig] = node;
+                } else {
+                    p.nodeNext[orig] = node;
+                    if (smemHist) {
+                        atomicAdd(&S.hist[node], 1u);
+                    } else {
+                        atomicAdd(&p.binCount[node], 1u);
+                    }
+                }
+            }
+        };
+        auto doA = [&](uint32_t t) -> bool {
+            const uint32_t buf = t & 1u;
+            if (!mbarWait(&S.accA[buf], (t >> 1) & 1u, abortFlag, p.err, 30)) return false;
+            tcFenceAfter();
+            uint32_t r[16];
+            tmemLoad16(tRow + buf * 256u, r);
+            tmemWaitTie(r);
+            tcFenceBefore();
+            mbarArrive(&S.accAFree[buf]);
+            const TileInfo ti = getTile(p, t0 + t);
+            const uint32_t b = argminScores(r, p.cnorm + (p.lbA + ti.group) * kMaxBranch);
+            if (two) {
+                if (buf) bstar1 = b; else bstar0 = b;
+            } else {
+                finalize(ti, ti.group * p.B + b);
+            }
+            return true;
+        };
+        auto doB = [&](uint32_t t) -> bool {
+            const uint32_t buf = t & 1u;
+            const uint32_t bs = buf ? bstar1 : bstar0;
+            if (!mbarWait(&S.accB[buf], (t >> 1) & 1u, abortFlag, p.err, 31)) return false;
+            tcFenceAfter();
+            uint32_t sel[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) sel[i] = 0;
+            for (uint32_t k = 0; k < p.B; k += 2) {
+                uint32_t r0[16], r1[16];
+                tmemLoad16(tRow + buf * 256u + 16u * k, r0);
+                if (k + 1 < p.B) tmemLoad16(tRow + buf * 256u + 16u * (k + 1), r1);
+                tmemWaitTie(r0);
+                tieRegs(r1);
+#pragma unroll
+                for (int i = 0; i < 16; i++) sel[i] = (bs == k) ? r0[i] : sel[i];
+                if (k + 1 < p.B) {
+#pragma unroll
+                    for (int i = 0; i < 16; i++) sel[i] = (bs == k + 1) ? r1[i] : sel[i];
+                }
+            }
+            tcFenceBefore();
+            mbarArrive(&S.accBFree[buf]);
+            const TileInfo ti = getTile(p, t0 + t);
+            const uint64_t child = uint64_t(ti.group) * p.B + bs; // in-level index at level 2p+1
+            const uint32_t b2 = argminScores(sel, p.cnorm + (p.lbB + child) * kMaxBranch);
+            finalize(ti, static_cast<uint32_t>(child * p.B + b2));
+            return true;
+        };
+        bool ok = true;
+        if (two) {
+            ok = doA(0);
+            for (uint32_t t = 0; ok && t < nT; t++) {
+                if (t + 1 < nT) ok = doA(t + 1);
+                if (ok) ok = doB(t);
+            }
+        } else {
+            for (uint32_t t = 0; ok && t < nT; t++) ok = doA(t);
+        }
+    }
+
+    tcFenceBefore();
+    __syncthreads();
+    if (smemHist) {
+        for (uint32_t i = threadIdx.x; i < p.nbBins; i += blockDim.x) {
+            const uint32_t v = S.hist[i];
+            if (v) atomicAdd(&p.binCount[i], v);
+        }
+    }
+    if (warp == 0) {
+        tcFenceAfter();
+        tmemDealloc(tmem, kTmemCols);
+    }
+}
+
+// ------------------------------------------------------------------ regroup kernels
+// Exclusive scans of the bin histogram: rowOff = scan(count), tileOff = scan(ceil(count/128));
+// totals[0] = number of tiles, totals[1] = number of rows.
+__global__ void __launch_bounds__(1024) scanBins(const uint32_t* count, uint32_t nb, uint32_t* rowOff,
+                                                 uint32_t* tileOff, uint32_t* totals)
+{
+    __shared__ uint32_t wa[32], wb[32];
+    __shared__ uint32_t carryA, carryB;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, w = tid >> 5;
+    if (tid == 0) {
+        carryA = 0;
+        carryB = 0;
+    }
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += 1024) {
+        const uint32_t i = base + tid;
+        const uint32_t c = i < nb ? count[i] : 0u;
+        const uint32_t tc = (c + kTileRows - 1) / kTileRows;
+        uint32_t a = c, b = tc;
+#pragma unroll
+        for (uint32_t off = 1; off < 32; off <<= 1) {
+            const uint32_t xa = __shfl_up_sync(0xFFFFFFFFu, a, off);
+            const uint32_t xb = __shfl_up_sync(0xFFFFFFFFu, b, off);
+            if (lane >= off) {
+                a += xa;
+                b += xb;
+            }
+        }
+        if (lane == 31) {
+            wa[w] = a;
+            wb[w] = b;
+        }
+        __syncthreads();
+        if (w == 0) {
+            uint32_t va = wa[lane], vb = wb[lane];
+#pragma unroll
+            for (uint32_t off = 1; off < 32; off <<= 1) {
+                const uint32_t xa = __shfl_up_sync(0xFFFFFFFFu, va, off);
+                const uint32_t xb = __shfl_up_sync(0xFFFFFFFFu, vb, off);
+                if (lane >= off) {
+                    va += xa;
+                    vb += xb;
+                }
+            }
+            wa[lane] = va; // inclusive over warps
+            wb[lane] = vb;
+        }
+        __syncthreads();
+        const uint32_t prevA = (w ? wa[w - 1] : 0u) + carryA;
+        const uint32_t prevB = (w ? wb[w - 1] : 0u) + carryB;
+        if (i < nb) {
+            rowOff[i] = prevA + a - c;
+            tileOff[i] = prevB + b - tc;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            carryA += wa[31];
+            carryB += wb[31];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        totals[0] = carryB;
+        totals[1] = carryA;
+    }
+}
+
+// One thread per tile: find its bin (last bin with tileOff <= t) and describe its rows.
+__global__ void buildTiles(const uint32_t* count, const uint32_t* rowOff, const uint32_t* tileOff, uint32_t nb,
+                           const uint32_t* totals, uint32_t maxTiles, TileInfo* tiles)
+{
+    const uint32_t nTiles = totals[0];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nTiles && t < maxTiles;
+         t += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nb; // first bin with tileOff > t
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (tileOff[mid] <= t) lo = mid + 1; else hi = mid;
+        }
+        const uint32_t g = lo - 1;
+        const uint32_t k = t - tileOff[g];
+        const uint32_t c = count[g] - k * kTileRows;
+        tiles[t] = TileInfo{g, rowOff[g] + k * kTileRows, c < kTileRows ? c : kTileRows, 0u};
+    }
+}
+
+constexpr uint32_t kScatterThreads = 256;
+constexpr uint32_t kScatterPerThread = 16;
+
+// perm[rowOff[node] + rank] = i for every descriptor i (order inside a bin is unspecified).
+__global__ void __launch_bounds__(kScatterThreads) scatterRows(const uint32_t* nodeNext, uint64_t n, uint32_t nb,
+                                                               const uint32_t* rowOff, uint32_t* cursor, uint32_t* perm)
+{
+    __shared__ uint32_t hist[kSmemHistMax];
+    const uint64_t base = uint64_t(blockIdx.x) * kScatterThreads * kScatterPerThread;
+    if (nb <= kSmemHistMax) {
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        uint32_t node[kScatterPerThread], rank[kScatterPerThread];
+#pragma unroll
+        for (uint32_t k = 0; k < kScatterPerThread; k++) {
+            const uint64_t i = base + uint64_t(k) * kScatterThreads + threadIdx.x;
+            node[k] = i < n ? __ldg(nodeNext + i) : 0xFFFFFFFFu;
+            rank[k] = node[k] != 0xFFFFFFFFu ? atomicAdd(&hist[node[k]], 1u) : 0u;
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+            const uint32_t c = hist[i];
+            hist[i] = c ? atomicAdd(&cursor[i], c) : 0u;
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t k = 0; k < kScatterPerThread; k++) {
+            const uint64_t i = base + uint64_t(k) * kScatterThreads + threadIdx.x;
+            if (node[k] != 0xFFFFFFFFu) perm[rowOff[node[k]] + hist[node[k]] + rank[k]] = static_cast<uint32_t>(i);
+        }
+    } else {
+#pragma unroll
+        for (uint32_t k = 0; k < kScatterPerThread; k++) {
+            const uint64_t i = base + uint64_t(k) * kScatterThreads + threadIdx.x;
+            if (i < n) {
+                const uint32_t nd = __ldg(nodeNext + i);
+                perm[rowOff[nd] + atomicAdd(&cursor[nd], 1u)] = static_cast<uint32_t>(i);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ plain FP32 SIMT kernel
+constexpr uint32_t kSimtDesc = 16; // descriptors per CTA, 16 threads each
+
+__device__ __forceinline__ float byteToFloat(uint32_t word, uint32_t k)
+{
+    // 0x4B0000bb is the float 2^23 + bb; subtracting 2^23 leaves bb exactly.
+    return __int_as_float(static_cast<int>(__byte_perm(word, 0x4B000000u, 0x7540u | k))) - 8388608.0f;
+}
+
+__global__ void __launch_bounds__(256) lookupSimtF32(const uint8_t* __restrict__ centers,
+                                                     const int32_t* __restrict__ cnorm, uint32_t B, uint32_t L,
+                                                     const uint8_t* __restrict__ desc, uint64_t n,
+                                                     uint32_t* __restrict__ out)
+{
+    __shared__ float xs[kSimtDesc][kDims + 4];
+    const uint32_t g = threadIdx.x / 16, j = threadIdx.x % 16;
+    const uint64_t descBase = uint64_t(blockIdx.x) * kSimtDesc;
+    if (threadIdx.x < kSimtDesc * 8) {
+        const uint32_t d = threadIdx.x / 8, part = threadIdx.x % 8;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (descBase + d < n) v = __ldg(reinterpret_cast<const uint4*>(desc + (descBase + d) * kDims) + part);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (uint32_t q = 0; q < 4; q++)
+#pragma unroll
+            for (uint32_t k = 0; k < 4; k++) xs[d][part * 16 + q * 4 + k] = byteToFloat(w[q], k);
+    }
+    __syncthreads();
+    uint64_t idx = 0, lb = 0;
+    for (uint32_t level = 0; level < L; level++) {
+        const uint64_t node = lb + idx;
+        const uint4* c = reinterpret_cast<const uint4*>(centers + (node * kMaxBranch + j) * kDims);
+        float acc = 0.f;
+#pragma unroll
+        for (uint32_t part = 0; part < 8; part++) {
+            const uint4 v = __ldg(c + part);
+            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (uint32_t q = 0; q < 4; q++)
+#pragma unroll
+                for (uint32_t k = 0; k < 4; k++) acc = fmaf(xs[g][part * 16 + q * 4 + k], byteToFloat(w[q], k), acc);
+        }
+        float s = j < B ? static_cast<float>(__ldg(cnorm + node * kMaxBranch + j)) - 2.f * acc : INFINITY;
+        uint32_t bj = j;
+#pragma unroll
+        for (uint32_t off = 8; off > 0; off >>= 1) {
+            const float os = __shfl_xor_sync(0xFFFFFFFFu, s, off, 16);
+            const uint32_t oj = __shfl_xor_sync(0xFFFFFFFFu, bj, off, 16);
+            if (os < s || (os == s && oj < bj)) {
+                s = os;
+                bj = oj;
+            }
+        }
+        idx = idx * B + bj;
+        lb = lb * B + 1;
+    }
+    if (j == 0 && descBase + g < n) out[descBase + g] = static_cast<uint32_t>(idx);
+}
+
+// ------------------------------------------------------------------ host side
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encodeTiledFn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        }
+    });
+    if (fn == nullptr) throw Error(kCudaError, "cuTensorMapEncodeTiled is unavailable");
+    return fn;
+}
+
+CUtensorMap makeRowMap(const uint8_t* desc, uint64_t n, uint32_t boxRows)
+{
+    CUtensorMap m{};
+    const cuuint64_t dims[2] = {kDims, n};
+    const cuuint64_t strides[1] = {kDims};
+    const cuuint32_t box[2] = {kDims, boxRows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encodeTiledFn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(desc), dims, strides,
+                                       box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(kCudaError, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+    return m;
+}
+
+int smCount()
+{
+    static int sms = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0;
+        RBW_CUDA(cudaGetDevice(&dev));
+        RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    });
+    return sms;
+}
+
+uint32_t maxBinsFor(uint32_t B, uint32_t L)
+{
+    uint64_t m = 1;
+    const uint32_t passes = (L + 1) / 2;
+    for (uint32_t p = 0; p + 1 < passes; p++) m = std::max<uint64_t>(m, ipow(B, 2 * p + 2));
+    return static_cast<uint32_t>(m);
+}
+
+} // namespace
+
+size_t lookupScratchBytes(uint32_t B, uint32_t L, uint64_t n)
+{
+    if (L <= 2) return 256; // single pass: no regroup (only the error record)
+    const uint64_t bins = maxBinsFor(B, L);
+    const uint64_t tiles = n / kTileRows + bins + 1;
+    auto a = [](uint64_t b) { return (b + 255) / 256 * 256; };
+    return a(sizeof(DeviceErrors)) + 2 * a(n * 4) + a((4 * bins + 4) * 4) + a(tiles * sizeof(TileInfo));
+}
+
+LookupScratch carveLookupScratch(void* base, uint32_t B, uint32_t L, uint64_t n)
+{
+    LookupScratch s{};
+    auto a = [](uint64_t b) { return (b + 255) / 256 * 256; };
+    uint8_t* p = static_cast<uint8_t*>(base);
+    s.err = reinterpret_cast<DeviceErrors*>(p);
+    p += a(sizeof(DeviceErrors));
+    if (L <= 2) return s;
+    const uint64_t bins = maxBinsFor(B, L);
+    s.nodeNext = reinterpret_cast<uint32_t*>(p);
+    p += a(n * 4);
+    s.perm = reinterpret_cast<uint32_t*>(p);
+    p += a(n * 4);
+    s.bins = reinterpret_cast<uint32_t*>(p);
+    p += a((4 * bins + 4) * 4);
+    s.tiles = p;
+    return s;
+}
+
+uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, uint32_t* leaf, LookupAlgo algo,
+                      const LookupScratch& scratch, cudaStream_t stream)
+{
+    if (n == 0) return 0;
+    if (algo == kLookupSimtF32) {
+        const uint64_t blocks = (n + kSimtDesc - 1) / kSimtDesc;
+        lookupSimtF32<<<static_cast<uint32_t>(blocks), 256, 0, stream>>>(tree.centers, tree.cnorm, tree.B, tree.L, desc,
+                                                                         n, leaf);
+        RBW_CUDA(cudaGetLastError());
+        return 1;
+    }
+    static std::once_flag attrOnce;
+    std::call_once(attrOnce, [] {
+        RBW_CUDA(cudaFuncSetAttribute(lookupPassTc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kTcSmemBytes)));
+    });
+    const CUtensorMap tmapTile = makeRowMap(desc, n, kTileRows);
+    const CUtensorMap tmapRow = makeRowMap(desc, n, 1);
+    const uint32_t B = tree.B, L = tree.L;
+    const uint32_t passes = (L + 1) / 2;
+    const uint32_t grid = static_cast<uint32_t>(smCount());
+    const uint64_t bins = L > 2 ? maxBinsFor(B, L) : 0;
+    uint32_t* count = scratch.bins;
+    uint32_t* rowOff = count ? count + bins : nullptr;
+    uint32_t* tileOff = count ? rowOff + bins : nullptr;
+    uint32_t* cursor = count ? tileOff + bins : nullptr;
+    uint32_t* totals = count ? cursor + bins : nullptr;
+    TileInfo* tiles = static_cast<TileInfo*>(scratch.tiles);
+    const uint32_t maxTiles = static_cast<uint32_t>(n / kTileRows + bins + 1);
+    uint32_t kernels = 0;
+    for (uint32_t pass = 0; pass < passes; pass++) {
+        PassParams p{};
+        p.centersSw = tree.centersSw;
+        p.cnorm = tree.cnorm;
+        p.B = B;
+        p.twoLevels = (2 * pass + 1 < L) ? 1u : 0u;
+        p.lbA = levelBeg(B, 2 * pass);
+        p.lbB = levelBeg(B, 2 * pass + 1);
+        p.nRows = n;
+        p.isFinal = pass + 1 == passes;
+        p.err = scratch.err;
+        if (pass > 0) {
+            p.perm = scratch.perm;
+            p.tiles = tiles;
+            p.nTilesDev = totals;
+        }
+        uint32_t nbBins = 0;
+        if (p.isFinal) {
+            p.out = leaf;
+        } else {
+            nbBins = static_cast<uint32_t>(ipow(B, 2 * pass + 2));
+            p.nodeNext = scratch.nodeNext;
+            p.binCount = count;
+            p.nbBins = nbBins;
+            RBW_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t) * nbBins, stream));
+        }
+        lookupPassTc<<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, tmapRow, p);
+        RBW_CUDA(cudaGetLastError());
+        kernels++;
+        if (!p.isFinal) {
+            scanBins<<<1, 1024, 0, stream>>>(count, nbBins, rowOff, tileOff, totals);
+            RBW_CUDA(cudaGetLastError());
+            const uint32_t tileBlocks = std::min<uint32_t>((maxTiles + 255) / 256, 4096);
+            buildTiles<<<tileBlocks, 256, 0, stream>>>(count, rowOff, tileOff, nbBins, totals, maxTiles, tiles);
+            RBW_CUDA(cudaGetLastError());
+            RBW_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nbBins, stream));
+            const uint64_t per = uint64_t(kScatterThreads) * kScatterPerThread;
+            scatterRows<<<static_cast<uint32_t>((n + per - 1) / per), kScatterThreads, 0, stream>>>(
+                scratch.nodeNext, n, nbBins, rowOff, cursor, scratch.perm);
+            RBW_CUDA(cudaGetLastError());
+            kernels += 3;
+        }
+    }
+    return kernels;
+}
+
+} // namespace rbw

@@ -1,0 +1,526 @@
+// Vocabulary: tree storage, GPU hierarchical k-means build, lookup dispatch and the blob format.
+//   build        : Vocabulary.cpp:32-121 + kmeans.cpp:27-343, all nodes of a level per launch
+//   lookup       : Vocabulary.h:59-63 / Vocabulary.cpp:162-173
+//   serialize    : Vocabulary.cpp:175-198 (byte-compatible for B = 16)
+//   deserialize  : Vocabulary.cpp:126-157
+#include "vocabulary.h"
+#include "kmeans.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <mutex>
+#include <random>
+#include <unordered_set>
+
+namespace rbw {
+
+DeviceBuffer::~DeviceBuffer()
+{
+    if (mPtr) cudaFree(mPtr);
+}
+
+void DeviceBuffer::reset(size_t bytes)
+{
+    if (mPtr) {
+        cudaFree(mPtr);
+        mPtr = nullptr;
+        mBytes = 0;
+    }
+    if (bytes) {
+        RBW_CUDA(cudaMalloc(&mPtr, bytes));
+        mBytes = bytes;
+    }
+}
+
+namespace {
+
+constexpr uint32_t kBlobExtMagic = 0x32574252u; // "RBW2": blobs with B != 16
+
+__global__ void swizzleKernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, uint64_t nbNodes)
+{
+    // 128-byte swizzle of every 8-row atom: row r's 16-byte chunk c lands at chunk c ^ (r & 7),
+    // the layout a TMA SWIZZLE_128B copy would write into 1024-byte-aligned shared memory.
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nbNodes * kMaxBranch * 8) return;
+    const uint32_t chunk = i % 8;
+    const uint64_t rowIdx = i / 8;
+    const uint32_t row = rowIdx % kMaxBranch;
+    const uint4 v = reinterpret_cast<const uint4*>(src)[i];
+    reinterpret_cast<uint4*>(dst + rowIdx * kDims)[chunk ^ (row & 7u)] = v;
+}
+
+__global__ void normsKernel(const uint8_t* __restrict__ centers, int32_t* __restrict__ cnorm, uint64_t nbNodes,
+                            uint32_t B)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nbNodes * kMaxBranch) return;
+    if (i % kMaxBranch >= B) {
+        cnorm[i] = kPadNorm;
+        return;
+    }
+    const uint4* c = reinterpret_cast<const uint4*>(centers + i * kDims);
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const uint4 v = c[k];
+        acc = __dp4a(v.x, v.x, acc);
+        acc = __dp4a(v.y, v.y, acc);
+        acc = __dp4a(v.z, v.z, acc);
+        acc = __dp4a(v.w, v.w, acc);
+    }
+    cnorm[i] = static_cast<int32_t>(acc);
+}
+
+__global__ void padKernel(const uint8_t* __restrict__ canon, uint8_t* __restrict__ padded, uint64_t nbNodes, uint32_t B)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; // (node, slot, chunk)
+    if (i >= nbNodes * kMaxBranch * 8) return;
+    const uint32_t chunk = i % 8;
+    const uint32_t b = (i / 8) % kMaxBranch;
+    const uint64_t node = i / (8 * kMaxBranch);
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (b < B) v = reinterpret_cast<const uint4*>(canon + (node * B + b) * kDims)[chunk];
+    reinterpret_cast<uint4*>(padded)[i] = v;
+}
+
+__global__ void iotaKernel(uint32_t* p, uint64_t n)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = static_cast<uint32_t>(i);
+}
+
+uint32_t blocksFor(uint64_t n, uint32_t t) { return static_cast<uint32_t>((n + t - 1) / t); }
+
+// The reference's initial pick (kmeans.cpp:260-287): min(n, k) distinct members drawn from one
+// default-seeded std::mt19937_64 that lives for the whole build (a fresh thread's
+// thread_local engine), sorted and padded with the last pick.  The steps -- `rng() % n` into a
+// hash set when n > 16*k, std::shuffle of 0..n-1 otherwise -- have to be the same calls on the
+// same standard-library engine to reproduce the reference's trees.
+uint32_t referencePick(std::mt19937_64& rng, uint32_t* dst, uint32_t space, uint32_t k)
+{
+    const uint32_t nbPick = std::min(space, k);
+    if (nbPick * 16 < space) {
+        std::unordered_set<uint32_t> picked;
+        while (picked.size() != nbPick) picked.insert(static_cast<uint32_t>(rng() % space));
+        std::copy_n(picked.begin(), nbPick, dst);
+    } else {
+        std::vector<uint32_t> all(space);
+        std::iota(all.begin(), all.end(), 0u);
+        std::shuffle(all.begin(), all.end(), rng);
+        std::copy_n(all.begin(), nbPick, dst);
+    }
+    std::sort(dst, dst + nbPick);
+    if (nbPick < k) std::fill(dst + nbPick, dst + k, nbPick != 0 ? dst[nbPick - 1] : 0u);
+    return nbPick;
+}
+
+float idfWeight(uint32_t nbDoc, uint32_t occ)
+{
+    // Vocabulary.cpp:202-207
+    return occ == 0 ? std::numeric_limits<float>::min()
+                    : std::max(std::numeric_limits<float>::min(), std::log(float(nbDoc) / float(occ)));
+}
+
+} // namespace
+
+void Vocabulary::allocate(uint32_t B, uint32_t L)
+{
+    if (B < 2 || B > kMaxBranch) throw Error(kUnsupported, "branch factor must be in [2, 16]");
+    if (L < 1 || L > 8) throw Error(kUnsupported, "number of levels must be in [1, 8]");
+    const uint64_t nodes = levelBeg(B, L);
+    if (ipow(B, L) > 0xFFFFFFFFull) throw Error(kUnsupported, "leaf index does not fit 32 bits");
+    mB = B;
+    mL = L;
+    mNbNodes = nodes;
+    mCenters.reset(nodes * kMaxBranch * kDims);
+    mCentersSw.reset(nodes * kMaxBranch * kDims);
+    mCnorm.reset(nodes * kMaxBranch * sizeof(int32_t));
+    mErrors.reset(sizeof(DeviceErrors));
+    RBW_CUDA(cudaMemset(mErrors.get(), 0, sizeof(DeviceErrors)));
+    mTree = DeviceTree{B, L, nodes, mCenters.as<uint8_t>(), mCentersSw.as<uint8_t>(), mCnorm.as<int32_t>()};
+}
+
+void Vocabulary::finalizeDevice(cudaStream_t stream)
+{
+    const uint64_t chunks = mNbNodes * kMaxBranch * 8;
+    swizzleKernel<<<blocksFor(chunks, 256), 256, 0, stream>>>(mCenters.as<uint8_t>(), mCentersSw.as<uint8_t>(),
+                                                              mNbNodes);
+    normsKernel<<<blocksFor(mNbNodes * kMaxBranch, 256), 256, 0, stream>>>(mCenters.as<uint8_t>(),
+                                                                           mCnorm.as<int32_t>(), mNbNodes, mB);
+    RBW_CUDA(cudaGetLastError());
+}
+
+std::unique_ptr<Vocabulary> Vocabulary::fromHost(uint32_t B, uint32_t L, const uint8_t* centers, const uint32_t* masks,
+                                                 const float* weights)
+{
+    std::unique_ptr<Vocabulary> v{new Vocabulary};
+    v->allocate(B, L);
+    const uint64_t nodes = v->mNbNodes;
+    DeviceBuffer canon(nodes * B * kDims);
+    RBW_CUDA(cudaMemcpy(canon.get(), centers, nodes * B * kDims, cudaMemcpyHostToDevice));
+    padKernel<<<blocksFor(nodes * kMaxBranch * 8, 256), 256>>>(canon.as<uint8_t>(), v->mCenters.as<uint8_t>(), nodes, B);
+    RBW_CUDA(cudaGetLastError());
+    v->mMasks.assign(masks, masks + nodes);
+    v->mWeights.assign(weights, weights + nodes * B);
+    v->finalizeDevice(nullptr);
+    RBW_CUDA(cudaDeviceSynchronize());
+    return v;
+}
+
+std::vector<uint8_t> Vocabulary::centersHost() const
+{
+    std::vector<uint8_t> padded(mNbNodes * kMaxBranch * kDims);
+    RBW_CUDA(cudaMemcpy(padded.data(), mCenters.get(), padded.size(), cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> out(mNbNodes * mB * kDims);
+    for (uint64_t n = 0; n < mNbNodes; n++)
+        std::memcpy(out.data() + n * mB * kDims, padded.data() + n * kMaxBranch * kDims, size_t(mB) * kDims);
+    return out;
+}
+
+const float* Vocabulary::levelWeights(uint32_t level) const
+{
+    if (level >= mL) throw Error(kInvalidArg, "level out of range");
+    return mWeights.data() + levelBeg(mB, level) * mB;
+}
+
+DeviceErrors Vocabulary::takeDeviceErrors() const
+{
+    DeviceErrors e{};
+    RBW_CUDA(cudaMemcpy(&e, mErrors.get(), sizeof(e), cudaMemcpyDeviceToHost));
+    RBW_CUDA(cudaMemset(mErrors.get(), 0, sizeof(e)));
+    return e;
+}
+
+cudaMemPool_t libraryPool()
+{
+    static cudaMemPool_t pools[64] = {};
+    static std::mutex mu;
+    int dev = 0;
+    RBW_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Error(kUnsupported, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(mu);
+    if (pools[dev] == nullptr) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        RBW_CUDA(cudaMemPoolCreate(&pools[dev], &props));
+        uint64_t keep = ~0ull;
+        RBW_CUDA(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return pools[dev];
+}
+
+uint32_t Vocabulary::lookup(const uint8_t* devDesc, uint64_t n, uint32_t* devLeaf, LookupAlgo algo,
+                            cudaStream_t stream, void* scratch, size_t scratchBytes) const
+{
+    if (n == 0) return 0;
+    if (devDesc == nullptr || devLeaf == nullptr) throw Error(kInvalidArg, "null buffer");
+    if (reinterpret_cast<uintptr_t>(devDesc) % 16 != 0)
+        throw Error(kInvalidArg, "descriptors must be 16-byte aligned");
+    if (algo == kLookupAuto) algo = kLookupTensorU8;
+    LookupScratch s{};
+    if (algo == kLookupSimtF32) {
+        s.err = mErrors.as<DeviceErrors>();
+        return launchLookup(mTree, devDesc, n, devLeaf, algo, s, stream);
+    }
+    // TMA row coordinates are signed 32-bit: process at most 2^30 rows per chunk.
+    const uint64_t chunk = std::min<uint64_t>(n, 1ull << 30);
+    const size_t need = lookupScratchBytes(mB, mL, chunk);
+    void* base = scratch;
+    bool owned = false;
+    if (base == nullptr) {
+        RBW_CUDA(cudaMallocFromPoolAsync(&base, need, libraryPool(), stream));
+        owned = true;
+    } else if (scratchBytes < need) {
+        throw Error(kInvalidArg, "lookup scratch too small");
+    }
+    s = carveLookupScratch(base, mB, mL, chunk);
+    s.err = mErrors.as<DeviceErrors>();
+    uint32_t kernels = 0;
+    for (uint64_t off = 0; off < n; off += chunk) {
+        kernels += launchLookup(mTree, devDesc + off * kDims, std::min(chunk, n - off), devLeaf + off, algo, s, stream);
+    }
+    if (owned) RBW_CUDA(cudaFreeAsync(base, stream));
+    return kernels;
+}
+
+uint32_t lookupHostPipelined(const Vocabulary& v, const uint8_t* hostDesc, uint64_t n, uint32_t* hostLeaf,
+                             LookupAlgo algo)
+{
+    if (n == 0) return 0;
+    if (hostDesc == nullptr || hostLeaf == nullptr) throw Error(kInvalidArg, "null buffer");
+    const uint64_t chunk = std::min<uint64_t>(n, 1ull << 20);
+    const size_t scratchBytes = lookupScratchBytes(v.branch(), v.levels(), chunk);
+    cudaMemPool_t pool = libraryPool();
+    cudaStream_t st[2] = {nullptr, nullptr};
+    void* dDesc[2] = {nullptr, nullptr};
+    void* dLeaf[2] = {nullptr, nullptr};
+    void* dScr[2] = {nullptr, nullptr};
+    uint32_t kernels = 0;
+    auto release = [&] {
+        for (int i = 0; i < 2; i++) {
+            if (st[i] == nullptr) continue;
+            if (dDesc[i]) cudaFreeAsync(dDesc[i], st[i]);
+            if (dLeaf[i]) cudaFreeAsync(dLeaf[i], st[i]);
+            if (dScr[i]) cudaFreeAsync(dScr[i], st[i]);
+            cudaStreamSynchronize(st[i]);
+            cudaStreamDestroy(st[i]);
+        }
+    };
+    try {
+        for (int i = 0; i < 2; i++) {
+            RBW_CUDA(cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking));
+            RBW_CUDA(cudaMallocFromPoolAsync(&dDesc[i], chunk * kDims, pool, st[i]));
+            RBW_CUDA(cudaMallocFromPoolAsync(&dLeaf[i], chunk * 4, pool, st[i]));
+            RBW_CUDA(cudaMallocFromPoolAsync(&dScr[i], scratchBytes, pool, st[i]));
+        }
+        uint64_t i = 0;
+        for (uint64_t off = 0; off < n; off += chunk, i++) {
+            const int k = static_cast<int>(i & 1);
+            const uint64_t cnt = std::min(chunk, n - off);
+            RBW_CUDA(cudaMemcpyAsync(dDesc[k], hostDesc + off * kDims, cnt * kDims, cudaMemcpyHostToDevice, st[k]));
+            kernels += v.lookup(static_cast<const uint8_t*>(dDesc[k]), cnt, static_cast<uint32_t*>(dLeaf[k]), algo,
+                                st[k], dScr[k], scratchBytes);
+            RBW_CUDA(cudaMemcpyAsync(hostLeaf + off, dLeaf[k], cnt * 4, cudaMemcpyDeviceToHost, st[k]));
+        }
+        for (int k = 0; k < 2; k++) RBW_CUDA(cudaStreamSynchronize(st[k]));
+    } catch (...) {
+        release();
+        throw;
+    }
+    release();
+    return kernels;
+}
+
+std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint8_t* devDesc, uint32_t nbDesc,
+                                              uint32_t nbDoc, const BuildOptions& opts, cudaStream_t stream,
+                                              BuildStats* stats)
+{
+    const auto tStart = std::chrono::steady_clock::now();
+    if (B < 2 || B > kMaxBranch) throw Error(kUnsupported, "branch factor must be in [2, 16]");
+    if (nbDesc < B) throw Error(kInvalidArg, "Insufficient descriptors"); // Vocabulary.cpp:38-40
+    if (nbDoc == 0) throw Error(kInvalidArg, "nbDoc must be positive");   // Vocabulary.cpp:41-43
+    if (devDesc == nullptr || reinterpret_cast<uintptr_t>(devDesc) % 16 != 0)
+        throw Error(kInvalidArg, "descriptors must be 16-byte aligned device memory");
+    if (opts.maxIterations == 0) throw Error(kInvalidArg, "maxIterations must be positive");
+    const uint32_t check = std::max(1u, opts.checkInterval);
+    std::unique_ptr<Vocabulary> voc{new Vocabulary};
+    voc->allocate(B, L);
+    RBW_CUDA(cudaMemsetAsync(voc->mCenters.get(), 0, voc->mCenters.bytes(), stream));
+    const uint64_t n = nbDesc;
+    const uint64_t maxLevelNodes = ipow(B, L - 1);
+    const uint64_t maxChildNodes = ipow(B, L);
+    const uint32_t maxTiles128 = static_cast<uint32_t>(n / 128 + maxLevelNodes + 1);
+    const uint32_t maxTiles32 = static_cast<uint32_t>(n / 32 + maxLevelNodes + 1);
+
+    DeviceBuffer members(n * 4), members2(n * 4), assign(n);
+    DeviceBuffer nodeCnt(std::max<uint64_t>(maxChildNodes, 1) * 4), nodeOff(std::max<uint64_t>(maxChildNodes, 1) * 4);
+    DeviceBuffer childCnt(maxChildNodes * 4), childOff(maxChildNodes * 4);
+    DeviceBuffer counts(maxLevelNodes * kMaxBranch * 4), sums(maxLevelNodes * kMaxBranch * kDims * 8);
+    DeviceBuffer changed(maxLevelNodes * 4), lastChanged(maxLevelNodes * 4), small(64);
+    DeviceBuffer picks(maxLevelNodes * B * 4), nValid(maxLevelNodes * 4);
+    DeviceBuffer tiles128(uint64_t(maxTiles128) * sizeof(NodeTile)), tiles32(uint64_t(maxTiles32) * sizeof(NodeTile));
+    DeviceBuffer tileOff(maxLevelNodes * 4);
+    DeviceBuffer scanTmp(scanTempWords(std::max<uint64_t>(uint64_t(B) * maxTiles32, maxLevelNodes)) * 4);
+    DeviceBuffer tileHist(uint64_t(B) * maxTiles32 * 4), tileScan(uint64_t(B) * maxTiles32 * 4);
+    uint32_t* totals = small.as<uint32_t>();
+    uint32_t* activeCount = small.as<uint32_t>() + 4;
+
+    iotaKernel<<<blocksFor(n, 256), 256, 0, stream>>>(members.as<uint32_t>(), n);
+    RBW_CUDA(cudaGetLastError());
+    const uint32_t zero = 0, n32 = nbDesc;
+    RBW_CUDA(cudaMemcpyAsync(nodeCnt.get(), &n32, 4, cudaMemcpyHostToDevice, stream));
+    RBW_CUDA(cudaMemcpyAsync(nodeOff.get(), &zero, 4, cudaMemcpyHostToDevice, stream));
+    RBW_CUDA(cudaMemsetAsync(counts.get(), 0, counts.bytes(), stream));
+    RBW_CUDA(cudaMemsetAsync(sums.get(), 0, sums.bytes(), stream));
+    RBW_CUDA(cudaMemsetAsync(changed.get(), 0, changed.bytes(), stream));
+
+    std::vector<uint32_t> occ(voc->mNbNodes * B, 0u);
+    voc->mMasks.assign(voc->mNbNodes, 0u);
+    std::mt19937_64 rng{}; // kmeans.cpp:264 (default seed)
+    std::vector<uint32_t> hostCnt, hostPicks, hostNValid;
+    if (stats) *stats = BuildStats{};
+
+    for (uint32_t level = 0; level < L; level++) {
+        const uint32_t nbLv = static_cast<uint32_t>(ipow(B, level));
+        const uint64_t lb = levelBeg(B, level);
+        KMeansLevel lv{};
+        lv.B = B;
+        lv.nbNodes = nbLv;
+        lv.nbMembers = n;
+        lv.desc = devDesc;
+        lv.members = members.as<uint32_t>();
+        lv.nodeOff = nodeOff.as<uint32_t>();
+        lv.nodeCnt = nodeCnt.as<uint32_t>();
+        lv.centers = voc->mCenters.as<uint8_t>() + lb * kMaxBranch * kDims;
+        lv.cnorm = voc->mCnorm.as<int32_t>() + lb * kMaxBranch;
+        lv.assign = assign.as<uint8_t>();
+        lv.counts = counts.as<uint32_t>();
+        lv.sums = sums.as<unsigned long long>();
+        lv.changed = changed.as<uint32_t>();
+        lv.lastChanged = lastChanged.as<uint32_t>();
+        lv.activeCount = activeCount;
+        lv.ieeeDivision = opts.ieeeDivision ? 1u : 0u;
+
+        // ---- initial centers
+        if (opts.initMode == kInitReference) {
+            hostCnt.resize(nbLv);
+            RBW_CUDA(cudaMemcpyAsync(hostCnt.data(), nodeCnt.get(), nbLv * 4, cudaMemcpyDeviceToHost, stream));
+            RBW_CUDA(cudaStreamSynchronize(stream));
+            hostPicks.resize(uint64_t(nbLv) * B);
+            for (uint32_t g = 0; g < nbLv; g++) {
+                const uint32_t k = referencePick(rng, hostPicks.data() + uint64_t(g) * B, hostCnt[g], B);
+                voc->mMasks[lb + g] = k >= 32 ? 0xFFFFFFFFu : ((1u << k) - 1u);
+            }
+            RBW_CUDA(cudaMemcpyAsync(picks.get(), hostPicks.data(), hostPicks.size() * 4, cudaMemcpyHostToDevice, stream));
+            launchInitCenters(lv, picks.as<uint32_t>(), n, stream);
+            RBW_CUDA(cudaStreamSynchronize(stream)); // hostPicks is reused next level
+        } else if (opts.initMode == kInitKMeansPP) {
+            launchKMeansPPInit(lv, opts.seed, level, nValid.as<uint32_t>(), stream);
+            hostNValid.resize(nbLv);
+            RBW_CUDA(cudaMemcpyAsync(hostNValid.data(), nValid.get(), nbLv * 4, cudaMemcpyDeviceToHost, stream));
+            RBW_CUDA(cudaStreamSynchronize(stream));
+            for (uint32_t g = 0; g < nbLv; g++) {
+                const uint32_t k = hostNValid[g];
+                voc->mMasks[lb + g] = k >= 32 ? 0xFFFFFFFFu : ((1u << k) - 1u);
+            }
+        } else {
+            if (opts.injected == nullptr) throw Error(kInvalidArg, "injected initialisation needs indices");
+            const uint32_t* inj = opts.injected + lb * B;
+            for (uint32_t g = 0; g < nbLv; g++) {
+                uint32_t k = 0;
+                for (uint32_t b = 0; b < B; b++) {
+                    const uint32_t v = inj[uint64_t(g) * B + b];
+                    if (v != kInvalidIdx && v >= n) throw Error(kInvalidArg, "injected index out of range");
+                    if (v != kInvalidIdx && b == k) k++;
+                }
+                voc->mMasks[lb + g] = k >= 32 ? 0xFFFFFFFFu : ((1u << k) - 1u);
+            }
+            RBW_CUDA(cudaMemcpyAsync(picks.get(), inj, uint64_t(nbLv) * B * 4, cudaMemcpyHostToDevice, stream));
+            launchInitCentersFromDesc(lv, picks.as<uint32_t>(), n, stream);
+            RBW_CUDA(cudaStreamSynchronize(stream));
+        }
+        launchCenterNorms(lv, stream);
+
+        // ---- Lloyd iterations (kmeans.cpp:237-252)
+        buildNodeTiles(lv.nodeCnt, lv.nodeOff, nbLv, 128, tileOff.as<uint32_t>(), scanTmp.as<uint32_t>(),
+                       tiles128.as<NodeTile>(), maxTiles128, totals, stream);
+        RBW_CUDA(cudaMemsetAsync(assign.get(), 0, n, stream)); // fresh (zeroed) assignment memory
+        RBW_CUDA(cudaMemsetAsync(lastChanged.get(), 0xFF, uint64_t(nbLv) * 4, stream));
+        uint32_t iters = 0;
+        for (uint32_t it = 0; it < opts.maxIterations; it++) {
+            launchAssign(lv, tiles128.as<NodeTile>(), totals, maxTiles128, stream);
+            RBW_CUDA(cudaMemsetAsync(activeCount, 0, 4, stream));
+            launchUpdate(lv, stream);
+            iters = it + 1;
+            if ((it + 1) % check == 0 || it + 1 == opts.maxIterations) {
+                uint32_t active = 0;
+                RBW_CUDA(cudaMemcpyAsync(&active, activeCount, 4, cudaMemcpyDeviceToHost, stream));
+                RBW_CUDA(cudaStreamSynchronize(stream));
+                if (active == 0) break;
+            }
+        }
+        if (stats && level < 16) stats->iterations[level] = iters;
+
+        // ---- stable regroup into the next level's nodes (Vocabulary.cpp:83-98)
+        RegroupScratch rs{tileHist.as<uint32_t>(), tileScan.as<uint32_t>(), scanTmp.as<uint32_t>(),
+                          tiles32.as<NodeTile>(), tileOff.as<uint32_t>(), totals, maxTiles32};
+        launchRegroup(lv, rs, members2.as<uint32_t>(), childCnt.as<uint32_t>(), childOff.as<uint32_t>(), stream);
+        RBW_CUDA(cudaMemcpyAsync(occ.data() + lb * B, childCnt.get(), uint64_t(nbLv) * B * 4, cudaMemcpyDeviceToHost,
+                                 stream));
+        std::swap(members, members2);
+        std::swap(nodeCnt, childCnt);
+        std::swap(nodeOff, childOff);
+    }
+    RBW_CUDA(cudaStreamSynchronize(stream));
+    voc->mWeights.resize(voc->mNbNodes * B);
+    for (size_t i = 0; i < occ.size(); i++) voc->mWeights[i] = idfWeight(nbDoc, occ[i]);
+    voc->finalizeDevice(stream);
+    RBW_CUDA(cudaStreamSynchronize(stream));
+    if (stats) {
+        stats->levels = L;
+        stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
+    }
+    return voc;
+}
+
+std::vector<uint8_t> Vocabulary::serialize() const
+{
+    const std::vector<uint8_t> c = centersHost();
+    const uint64_t nodes = mNbNodes;
+    std::vector<uint8_t> out;
+    if (mB == 16) {
+        // [u32 L][Node: uint32[32 words][16 centers] x nodes][u16 mask x nodes][float[16] x nodes]
+        out.resize(4 + nodes * (2048 + 2 + 64));
+        std::memcpy(out.data(), &mL, 4);
+        uint8_t* nodeBytes = out.data() + 4;
+        for (uint64_t n = 0; n < nodes; n++)
+            for (uint32_t j = 0; j < 16; j++)
+                for (uint32_t w = 0; w < 32; w++)
+                    std::memcpy(nodeBytes + n * 2048 + (w * 16 + j) * 4, c.data() + (n * 16 + j) * kDims + w * 4, 4);
+        uint8_t* maskBytes = nodeBytes + nodes * 2048;
+        for (uint64_t n = 0; n < nodes; n++) {
+            const uint16_t m = static_cast<uint16_t>(mMasks[n]);
+            std::memcpy(maskBytes + n * 2, &m, 2);
+        }
+        std::memcpy(maskBytes + nodes * 2, mWeights.data(), nodes * 64);
+    } else {
+        // [u32 magic][u32 B][u32 L][centers nodes x B x 128][u32 mask x nodes][float[B] x nodes]
+        out.resize(12 + nodes * mB * kDims + nodes * 4 + nodes * mB * 4);
+        const uint32_t hdr[3] = {kBlobExtMagic, mB, mL};
+        std::memcpy(out.data(), hdr, 12);
+        std::memcpy(out.data() + 12, c.data(), c.size());
+        std::memcpy(out.data() + 12 + c.size(), mMasks.data(), nodes * 4);
+        std::memcpy(out.data() + 12 + c.size() + nodes * 4, mWeights.data(), nodes * mB * 4);
+    }
+    return out;
+}
+
+std::unique_ptr<Vocabulary> Vocabulary::deserialize(const uint8_t* blob, size_t size)
+{
+    if (blob == nullptr || size < 4) throw Error(kInvalidBlob, "invalid blob");
+    uint32_t first = 0;
+    std::memcpy(&first, blob, 4);
+    if (first == kBlobExtMagic) {
+        if (size < 12) throw Error(kInvalidBlob, "invalid blob");
+        uint32_t B = 0, L = 0;
+        std::memcpy(&B, blob + 4, 4);
+        std::memcpy(&L, blob + 8, 4);
+        if (B < 2 || B > 16 || L < 1 || L > 8) throw Error(kInvalidBlob, "invalid blob");
+        const uint64_t nodes = levelBeg(B, L);
+        const uint64_t cBytes = nodes * B * kDims;
+        if (size != 12 + cBytes + nodes * 4 + nodes * B * 4) throw Error(kInvalidBlob, "invalid blob");
+        std::vector<uint32_t> masks(nodes);
+        std::vector<float> weights(nodes * B);
+        std::memcpy(masks.data(), blob + 12 + cBytes, nodes * 4);
+        std::memcpy(weights.data(), blob + 12 + cBytes + nodes * 4, nodes * B * 4);
+        return fromHost(B, L, blob + 12, masks.data(), weights.data());
+    }
+    const uint32_t L = first;
+    if (L < 1 || L > 7) throw Error(kInvalidBlob, "invalid blob");
+    const uint64_t nodes = levelBeg(16, L);
+    if (size != 4 + nodes * (2048 + 2 + 64)) throw Error(kInvalidBlob, "invalid blob"); // Vocabulary.cpp:142-144
+    const uint8_t* nodeBytes = blob + 4;
+    std::vector<uint8_t> canon(nodes * 16 * kDims);
+    for (uint64_t n = 0; n < nodes; n++)
+        for (uint32_t j = 0; j < 16; j++)
+            for (uint32_t w = 0; w < 32; w++)
+                std::memcpy(canon.data() + (n * 16 + j) * kDims + w * 4, nodeBytes + n * 2048 + (w * 16 + j) * 4, 4);
+    std::vector<uint32_t> masks(nodes);
+    const uint8_t* maskBytes = nodeBytes + nodes * 2048;
+    for (uint64_t n = 0; n < nodes; n++) {
+        uint16_t m = 0;
+        std::memcpy(&m, maskBytes + n * 2, 2);
+        masks[n] = m;
+    }
+    std::vector<float> weights(nodes * 16);
+    std::memcpy(weights.data(), maskBytes + nodes * 2, nodes * 64);
+    return fromHost(16, L, canon.data(), masks.data(), weights.data());
+}
+
+} // namespace rbw
