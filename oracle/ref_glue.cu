@@ -232,6 +232,33 @@ int ref_lookup(const uint8_t* blob, uint64_t blobSize, const uint8_t* hostDesc, 
     });
 }
 
+// Device time of the reference lookup kernel (launchVocTreeLookUp via IVocabulary::lookUp) on
+// descriptors already in device memory: `iters` launches bracketed by CUDA events.
+int ref_lookup_device_timed(const uint8_t* blob, uint64_t blobSize, const uint8_t* hostDesc, uint32_t nbDesc,
+                            uint32_t* hostOut, uint32_t iters, float* msPerLaunch)
+{
+    return guarded([&] {
+        const auto voc = rbow::deserializeVocabulary(blob, blobSize);
+        auto devDesc = allocCudaMem<uint8_t>(size_t(nbDesc) * 128 + 16);
+        auto devOut = allocCudaMem<uint32_t>(size_t(nbDesc) + 1);
+        cudaCheck(cudaMemcpy(devDesc.get(), hostDesc, size_t(nbDesc) * 128, cudaMemcpyHostToDevice));
+        voc->lookUp(devDesc.get(), nbDesc, devOut.get(), nullptr);
+        cudaEvent_t e0, e1;
+        cudaCheck(cudaEventCreate(&e0));
+        cudaCheck(cudaEventCreate(&e1));
+        cudaCheck(cudaEventRecord(e0, nullptr));
+        for (uint32_t i = 0; i < iters; i++) voc->lookUp(devDesc.get(), nbDesc, devOut.get(), nullptr);
+        cudaCheck(cudaEventRecord(e1, nullptr));
+        cudaCheck(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaCheck(cudaEventElapsedTime(&ms, e0, e1));
+        *msPerLaunch = ms / float(iters ? iters : 1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaCheck(cudaMemcpy(hostOut, devOut.get(), size_t(nbDesc) * 4, cudaMemcpyDeviceToHost));
+    });
+}
+
 // One reference assign + (optionally) update on a single k-means task, as
 // tests/KmeansAssignCenterTests.cpp:94-105,241-253 drive the kernels.
 //   tilesIn : DescTile layout, uint32[nbTiles][32 words][32 desc]

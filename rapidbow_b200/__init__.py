@@ -83,6 +83,9 @@ def load_library() -> C.CDLL:
         "rbw_voc_lookup_scratch_bytes": (C.c_int, [vp, u64, C.POINTER(u64)]),
         "rbw_voc_device_errors": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
         "rbw_voc_destroy": (None, [vp]),
+        "rbw_timing_enable": (None, [i32]),
+        "rbw_timing_reset": (C.c_int, []),
+        "rbw_timing_read": (C.c_int, [u32, C.POINTER(C.c_double), C.POINTER(u64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -245,6 +248,26 @@ class Vocabulary:
         buf = (C.c_uint8 * size.value)()
         _check(self._lib.rbw_voc_serialize(self._h, buf, size.value, C.byref(size)))
         return bytes(buf)
+
+
+TIMED_KERNELS = {"lookup_pass_tc": 0, "lookup_simt_f32": 1, "lookup_regroup": 2, "kmeans_assign": 3,
+                 "kmeans_update": 4, "score": 5, "index": 6}
+
+
+def timing_enable(on: bool) -> None:
+    """Brackets this library's kernel launches with CUDA events (see rbw_timing_enable)."""
+    load_library().rbw_timing_enable(1 if on else 0)
+
+
+def timing_reset() -> None:
+    _check(load_library().rbw_timing_reset())
+
+
+def timing_read(kernel: str):
+    """(total milliseconds, launches) of the completed launches of one kernel since the reset."""
+    ms, n = C.c_double(), C.c_uint64()
+    _check(load_library().rbw_timing_read(TIMED_KERNELS[kernel], C.byref(ms), C.byref(n)))
+    return ms.value, n.value
 
 
 def build_vocabulary(descriptors, branch_factor: int = 16, nb_doc: int = 1, nb_levels: int = 4, stream=None,

@@ -2,6 +2,7 @@
 // returns an rbw_status and leaves a message for rbw_last_error().
 #include "rapidbow_b200.h"
 #include "vocabulary.h"
+#include "timing.h"
 
 #include <cstring>
 #include <new>
@@ -203,5 +204,20 @@ int rbw_voc_device_errors(const rbw_vocabulary* voc, uint32_t* code, uint32_t* w
 }
 
 void rbw_voc_destroy(rbw_vocabulary* voc) { delete voc; }
+
+void rbw_timing_enable(int32_t on) { rbw::timingEnable(on != 0); }
+
+int rbw_timing_reset(void)
+{
+    return guard([] { rbw::timingReset(); });
+}
+
+int rbw_timing_read(uint32_t kernel, double* total_ms, uint64_t* launches)
+{
+    return guard([&] {
+        if (kernel >= rbw::kTimedCount) throw rbw::Error(rbw::kInvalidArg, "unknown kernel id");
+        rbw::timingRead(static_cast<rbw::TimedKernel>(kernel), total_ms, launches);
+    });
+}
 
 } // extern "C"

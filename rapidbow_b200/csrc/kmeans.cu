@@ -2,6 +2,7 @@
 // x.c_b from dp4a (u8 x u8 -> u32), argmin with the lowest index on ties (kmeans.cu:131-135).
 // Center sums are exact (u32 in shared memory, u64 in global memory).
 #include "kmeans.cuh"
+#include "timing.h"
 
 #include <algorithm>
 
@@ -539,6 +540,7 @@ void launchAssign(const KMeansLevel& lv, const NodeTile* tiles, const uint32_t* 
     RBW_CUDA(cudaGetDevice(&dev));
     RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const uint32_t grid = std::max(1u, std::min<uint32_t>(maxTiles, static_cast<uint32_t>(sms) * 8));
+    ScopedKernelTimer timer(kTimedAssign, s);
     assignKernel<<<grid, kAssignThreads, 0, s>>>(lv, tiles, nTilesDev);
     RBW_CUDA(cudaGetLastError());
 }

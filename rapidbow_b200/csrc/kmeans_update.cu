@@ -5,6 +5,7 @@
 // whenever the reference's sum does not overflow, i.e. below 2^32).  With ieeeDivision set the
 // quotient is the correctly rounded one instead (__fdiv_rn), which is what the CPU oracle computes.
 #include "kmeans.cuh"
+#include "timing.h"
 
 namespace rbw {
 namespace {
@@ -61,6 +62,7 @@ __global__ void __launch_bounds__(256) updateKernel(KMeansLevel lv)
 void launchUpdate(const KMeansLevel& lv, cudaStream_t s)
 {
     if (lv.nbNodes == 0) return;
+    ScopedKernelTimer timer(kTimedUpdate, s);
     updateKernel<<<lv.nbNodes, 256, 0, s>>>(lv);
     RBW_CUDA(cudaGetLastError());
 }

@@ -13,6 +13,7 @@
 //   * lookupSimtF32 : plain FP32 SIMT kernel (16 threads per descriptor, one center each),
 //                     the comparison baseline.  Exact for uint8 data (all sums < 2^24).
 #include "lookup.cuh"
+#include "timing.h"
 
 #include <algorithm>
 #include <mutex>
@@ -27,15 +28,22 @@ struct TileInfo {
     uint32_t pad;
 };
 
-constexpr uint32_t kStages = 4;
+constexpr uint32_t kStages = 8;
 constexpr uint32_t kTileRows = 128;
 constexpr uint32_t kTileBytes = kTileRows * kDims;    // 16 KB
 constexpr uint32_t kNodeBytes = kMaxBranch * kDims;   // 2 KB: one node's 16 centers
 constexpr uint32_t kBBlockBytes = kNodeBytes * 17;    // node + up to 16 children
-constexpr uint32_t kTcThreads = 192;                  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
-constexpr uint32_t kEpiThreads = 128;
-constexpr uint32_t kSmemHistMax = 4096;
-constexpr uint32_t kTmemCols = 512;                   // two accumulator buffers of 256 columns
+constexpr uint32_t kEpiWarpsPerRole = 4;              // one warp per TMEM lane quarter
+constexpr uint32_t kTcThreads = 32 * (2 + 2 * kEpiWarpsPerRole); // TMA, MMA, 4 A warps, 4 B warps
+constexpr uint32_t kSmemHistMax = 1024;
+constexpr uint32_t kTmemCols = 512;                   // children block [0,256), level-2p blocks at 256, 272
+constexpr uint32_t kTmemA = 256;
+constexpr uint32_t kTileCache = 1024;
+constexpr uint32_t kGatherDepth = 4;                  // gathered tiles in flight (< kStages)
+// Branch hand-off ring between A and B warps.  The A warps write tile t + kBsSlots only after the
+// level-2p MMA of that tile, which follows the children MMA of tile t + 2, which waits for the
+// B warps to release tile t + 1 -- so 4 slots never overwrite a tile the B warps still read.
+constexpr uint32_t kBsSlots = 4;
 
 struct TcSmem {
     uint8_t a[kStages][kTileBytes];
@@ -44,18 +52,24 @@ struct TcSmem {
     uint64_t aEmpty[kStages];
     uint64_t bFull[2];
     uint64_t bEmpty[2];
-    uint64_t accA[2];
-    uint64_t accAFree[2];
-    uint64_t accB[2];
-    uint64_t accBFree[2];
+    uint64_t accA[2];     // level-2p accumulators j complete
+    uint64_t accAFree[2]; // A warps done with level-2p buffer j
+    uint64_t accB;        // children accumulators complete (one phase per tile)
+    uint64_t accBFree;    // B warps done with the children buffer
+    uint64_t bsReady[kBsSlots]; // A warps wrote the branches of tile t into bstar[t % kBsSlots]
     uint64_t mmaDone;
     uint32_t tmemBase;
     uint32_t abortFlag;
+    alignas(16) int32_t cn[2][17][16]; // |c|^2 of each B slot: row 0 = node, rows 1.. = children
     uint32_t hist[kSmemHistMax];
+    TileInfo tileCache[kTileCache];    // this CTA's tile list (passes after the first)
+    alignas(16) int32_t idx[kGatherDepth][kTileRows]; // gather row indices, ring
+    uint8_t bstar[kBsSlots][kTileRows];             // level-2p branch per row, A -> B warps
 };
 constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 1024;
 
 struct PassParams {
+    const uint8_t* desc;     // [nRows][128] descriptors (gathered passes)
     const uint8_t* centersSw;
     const int32_t* cnorm;
     uint32_t B;
@@ -95,22 +109,30 @@ __device__ __forceinline__ void tmemWaitTie(uint32_t (&r)[16])
                  :
                  : "memory");
 }
-__device__ __forceinline__ void tieRegs(uint32_t (&r)[16])
+// 32 lanes x 128 columns of 32-bit accumulators.
+__device__ __forceinline__ void tmemLoad128(uint32_t taddr, uint32_t (&r)[128])
 {
-    asm volatile(""
-                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
-                   "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]),
-                   "+r"(r[14]), "+r"(r[15]));
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x128.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63, %64, %65, %66, %67, %68, %69, %70, %71, %72, %73, %74, %75, %76, %77, %78, %79, %80, %81, %82, %83, %84, %85, %86, %87, %88, %89, %90, %91, %92, %93, %94, %95, %96, %97, %98, %99, %100, %101, %102, %103, %104, %105, %106, %107, %108, %109, %110, %111, %112, %113, %114, %115, %116, %117, %118, %119, %120, %121, %122, %123, %124, %125, %126, %127}, [%128];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63]), "=r"(r[64]), "=r"(r[65]), "=r"(r[66]), "=r"(r[67]), "=r"(r[68]), "=r"(r[69]), "=r"(r[70]), "=r"(r[71]), "=r"(r[72]), "=r"(r[73]), "=r"(r[74]), "=r"(r[75]), "=r"(r[76]), "=r"(r[77]), "=r"(r[78]), "=r"(r[79]), "=r"(r[80]), "=r"(r[81]), "=r"(r[82]), "=r"(r[83]), "=r"(r[84]), "=r"(r[85]), "=r"(r[86]), "=r"(r[87]), "=r"(r[88]), "=r"(r[89]), "=r"(r[90]), "=r"(r[91]), "=r"(r[92]), "=r"(r[93]), "=r"(r[94]), "=r"(r[95]), "=r"(r[96]), "=r"(r[97]), "=r"(r[98]), "=r"(r[99]), "=r"(r[100]), "=r"(r[101]), "=r"(r[102]), "=r"(r[103]), "=r"(r[104]), "=r"(r[105]), "=r"(r[106]), "=r"(r[107]), "=r"(r[108]), "=r"(r[109]), "=r"(r[110]), "=r"(r[111]), "=r"(r[112]), "=r"(r[113]), "=r"(r[114]), "=r"(r[115]), "=r"(r[116]), "=r"(r[117]), "=r"(r[118]), "=r"(r[119]), "=r"(r[120]), "=r"(r[121]), "=r"(r[122]), "=r"(r[123]), "=r"(r[124]), "=r"(r[125]), "=r"(r[126]), "=r"(r[127])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmemWaitTie128(uint32_t (&r)[128])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31]), "+r"(r[32]), "+r"(r[33]), "+r"(r[34]), "+r"(r[35]), "+r"(r[36]), "+r"(r[37]), "+r"(r[38]), "+r"(r[39]), "+r"(r[40]), "+r"(r[41]), "+r"(r[42]), "+r"(r[43]), "+r"(r[44]), "+r"(r[45]), "+r"(r[46]), "+r"(r[47]), "+r"(r[48]), "+r"(r[49]), "+r"(r[50]), "+r"(r[51]), "+r"(r[52]), "+r"(r[53]), "+r"(r[54]), "+r"(r[55]), "+r"(r[56]), "+r"(r[57]), "+r"(r[58]), "+r"(r[59]), "+r"(r[60]), "+r"(r[61]), "+r"(r[62]), "+r"(r[63]), "+r"(r[64]), "+r"(r[65]), "+r"(r[66]), "+r"(r[67]), "+r"(r[68]), "+r"(r[69]), "+r"(r[70]), "+r"(r[71]), "+r"(r[72]), "+r"(r[73]), "+r"(r[74]), "+r"(r[75]), "+r"(r[76]), "+r"(r[77]), "+r"(r[78]), "+r"(r[79]), "+r"(r[80]), "+r"(r[81]), "+r"(r[82]), "+r"(r[83]), "+r"(r[84]), "+r"(r[85]), "+r"(r[86]), "+r"(r[87]), "+r"(r[88]), "+r"(r[89]), "+r"(r[90]), "+r"(r[91]), "+r"(r[92]), "+r"(r[93]), "+r"(r[94]), "+r"(r[95]), "+r"(r[96]), "+r"(r[97]), "+r"(r[98]), "+r"(r[99]), "+r"(r[100]), "+r"(r[101]), "+r"(r[102]), "+r"(r[103]), "+r"(r[104]), "+r"(r[105]), "+r"(r[106]), "+r"(r[107]), "+r"(r[108]), "+r"(r[109]), "+r"(r[110]), "+r"(r[111]), "+r"(r[112]), "+r"(r[113]), "+r"(r[114]), "+r"(r[115]), "+r"(r[116]), "+r"(r[117]), "+r"(r[118]), "+r"(r[119]), "+r"(r[120]), "+r"(r[121]), "+r"(r[122]), "+r"(r[123]), "+r"(r[124]), "+r"(r[125]), "+r"(r[126]), "+r"(r[127])
+                 :
+                 : "memory");
 }
 
-// argmin_b (|c_b|^2 - 2 x.c_b), lowest b on ties (vocTreeLookUp.cu:108-125).
+// argmin_b (|c_b|^2 - 2 x.c_b), lowest b on ties (vocTreeLookUp.cu:108-125); cnormNode is the
+// node's 16 exact |c|^2 values in shared memory.
 __device__ __forceinline__ uint32_t argminScores(const uint32_t (&dot)[16], const int32_t* cnormNode)
 {
     const int4* cn4 = reinterpret_cast<const int4*>(cnormNode);
     int32_t cn[16];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const int4 v = __ldg(cn4 + i);
+        const int4 v = cn4[i];
         cn[4 * i] = v.x;
         cn[4 * i + 1] = v.y;
         cn[4 * i + 2] = v.z;
@@ -129,6 +151,32 @@ __device__ __forceinline__ uint32_t argminScores(const uint32_t (&dot)[16], cons
     return bi;
 }
 
+// Tile i of this CTA (first pass: computed; later passes: the staged copy of the tile list).
+__device__ __forceinline__ TileInfo tileAtSmem(const TcSmem& S, const PassParams& p, uint32_t t0, uint32_t i)
+{
+    if (p.tiles == nullptr) return getTile(p, t0 + i);
+    return i < kTileCache ? S.tileCache[i] : p.tiles[t0 + i];
+}
+__device__ __forceinline__ bool lastOfGroupSmem(const TcSmem& S, const PassParams& p, uint32_t t0, uint32_t nT,
+                                                uint32_t i, uint32_t g)
+{
+    return i + 1 >= nT || tileAtSmem(S, p, t0, i + 1).group != g;
+}
+// Writes one row's result: the leaf (last pass) or the next group's node + its histogram count.
+__device__ __forceinline__ void emitRow(TcSmem& S, const PassParams& p, bool smemHist, uint32_t orig, uint32_t node)
+{
+    if (p.isFinal) {
+        p.out[orig] = node;
+    } else {
+        p.nodeNext[orig] = node;
+        if (smemHist) {
+            atomicAdd(&S.hist[node], 1u);
+        } else {
+            atomicAdd(&p.binCount[node], 1u);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kTcThreads, 1)
     lookupPassTc(const __grid_constant__ CUtensorMap tmapTile, const __grid_constant__ CUtensorMap tmapRow,
                  const PassParams p)
@@ -144,6 +192,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t nT = t1 - t0;
     const bool smemHist = !p.isFinal && p.nbBins <= kSmemHistMax;
     const bool two = p.twoLevels != 0;
+    const bool gather = p.perm != nullptr;
     volatile uint32_t* abortFlag = &S.abortFlag;
 
     if (threadIdx.x == 0) {
@@ -153,18 +202,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         for (uint32_t j = 0; j < 2; j++) {
             mbarInit(&S.bFull[j], 1);
-            mbarInit(&S.bEmpty[j], 1);
+            mbarInit(&S.bEmpty[j], 1 + (two ? 2u : 1u) * kEpiWarpsPerRole); // MMA commit + epilogue warps
             mbarInit(&S.accA[j], 1);
-            mbarInit(&S.accAFree[j], kEpiThreads);
-            mbarInit(&S.accB[j], 1);
-            mbarInit(&S.accBFree[j], kEpiThreads);
+            mbarInit(&S.accAFree[j], kEpiWarpsPerRole);
         }
+        mbarInit(&S.accB, 1);
+        mbarInit(&S.accBFree, kEpiWarpsPerRole);
+        for (uint32_t j = 0; j < kBsSlots; j++) mbarInit(&S.bsReady[j], kEpiWarpsPerRole);
         mbarInit(&S.mmaDone, 1);
         S.abortFlag = 0;
         fenceMbarInit();
     }
     if (smemHist) {
         for (uint32_t i = threadIdx.x; i < p.nbBins; i += blockDim.x) S.hist[i] = 0;
+    }
+    if (p.tiles != nullptr) {
+        const uint32_t m = nT < kTileCache ? nT : kTileCache;
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) S.tileCache[i] = p.tiles[t0 + i];
     }
     if (warp == 0) {
         tmemAlloc(&S.tmemBase, kTmemCols);
@@ -174,26 +228,71 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     tcFenceAfter();
     const uint32_t tmem = S.tmemBase;
-
     if (nT > 0 && warp == 0) {
-        // ------------------------------------------------------------ TMA producer
-        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, slotUses[2] = {0, 0};
+        // ------------------------------------------------------------ producer
+        // First pass: one TMA tiled load (128 rows, 128-byte swizzle) per tile.
+        // Later passes: the tile's 128 rows are gathered with 16-byte cp.async (lane q copies rows
+        // 4q..4q+3, 8 chunks each) into the same swizzled layout, kGatherDepth tiles in flight.
+        // Row indices travel through a shared-memory ring inside the same copy groups: group #i
+        // (prologue for i < kGatherDepth, else committed by iteration i - kGatherDepth) carries
+        // the indices of tile i and the rows of tile i - kGatherDepth, so wait_group(depth - 1)
+        // at the top of iteration i completes both; those rows are then published to the MMA
+        // with a proxy fence (generic-proxy writes, async-proxy reader) and an arrival.
+        auto copyIdx = [&](uint32_t i) {
+            if (i < nT) {
+                const TileInfo ti = tileAtSmem(S, p, t0, i);
+#pragma unroll
+                for (uint32_t j = 0; j < 4; j++) {
+                    const uint32_t rr = 4 * lane + j;
+                    cpAsync4(&S.idx[i % kGatherDepth][rr], p.perm + ti.start + (rr < ti.count ? rr : 0u));
+                }
+            }
+        };
+        uint32_t published = 0; // tiles [0, published) are visible to the MMA
+        auto publishUpTo = [&](uint32_t end) {
+            if (published >= end) return;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                for (uint32_t j = published; j < end; j++) mbarArrive(&S.aFull[j % kStages]);
+            published = end;
+        };
+        if (gather) {
+            for (uint32_t d = 0; d < kGatherDepth; d++) {
+                copyIdx(d);
+                cpAsyncCommit();
+            }
+        }
+        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, slotUses0 = 0, slotUses1 = 0;
+        uint32_t issued = 0;
         for (uint32_t i = 0; i < nT; i++) {
-            const TileInfo ti = getTile(p, t0 + i);
+            const TileInfo ti = tileAtSmem(S, p, t0, i);
+            if (gather) {
+                cpAsyncWait<kGatherDepth - 1>();
+                if (i >= kGatherDepth) publishUpTo(i - kGatherDepth + 1);
+            }
             bool ok = true;
             if (ti.group != prevGroup) {
+                // A slot is released only after the MMA and epilogue are done with tile i-2 or
+                // earlier, so every gathered tile must be published before waiting for it.
+                if (gather) {
+                    cpAsyncWait<0>();
+                    publishUpTo(i);
+                }
                 slot ^= 1u;
-                const uint32_t k = slotUses[slot]++;
+                const uint32_t k = slot ? slotUses1++ : slotUses0++;
                 if (lane == 0) {
                     ok = mbarWait(&S.bEmpty[slot], (k & 1u) ^ 1u, abortFlag, p.err, 10);
                     if (ok) {
-                        const uint32_t bytes = kNodeBytes * (two ? 1u + p.B : 1u);
-                        mbarArriveExpectTx(&S.bFull[slot], bytes);
+                        const uint32_t nb = two ? p.B : 0u;
+                        mbarArriveExpectTx(&S.bFull[slot], (kNodeBytes + 64u) * (1u + nb));
                         bulkLoad(S.b[slot], p.centersSw + (p.lbA + ti.group) * kNodeBytes, kNodeBytes, &S.bFull[slot]);
+                        bulkLoad(&S.cn[slot][0][0], p.cnorm + (p.lbA + ti.group) * kMaxBranch, 64u, &S.bFull[slot]);
                         if (two) {
-                            bulkLoad(S.b[slot] + kNodeBytes,
-                                     p.centersSw + (p.lbB + uint64_t(ti.group) * p.B) * kNodeBytes, kNodeBytes * p.B,
+                            const uint64_t c0 = p.lbB + uint64_t(ti.group) * p.B;
+                            bulkLoad(S.b[slot] + kNodeBytes, p.centersSw + c0 * kNodeBytes, kNodeBytes * p.B,
                                      &S.bFull[slot]);
+                            bulkLoad(&S.cn[slot][1][0], p.cnorm + c0 * kMaxBranch, 64u * p.B, &S.bFull[slot]);
                         }
                     }
                 }
@@ -205,188 +304,209 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const uint32_t ph = (i / kStages) & 1u;
             if (lane == 0) {
                 ok = mbarWait(&S.aEmpty[s], ph ^ 1u, abortFlag, p.err, 11);
-                if (ok) mbarArriveExpectTx(&S.aFull[s], kTileBytes);
+                if (ok && !gather) mbarArriveExpectTx(&S.aFull[s], kTileBytes);
             }
             ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
             if (!ok) break;
-            if (p.perm == nullptr) {
+            if (!gather) {
                 if (lane == 0) tmaLoad2d(S.a[s], &tmapTile, 0, static_cast<int32_t>(ti.start), &S.aFull[s]);
             } else {
-                // lane q gathers rows 4q..4q+3 of the tile (rows past the group end repeat row 0).
-                int32_t r[4];
+                const int4 rows = *reinterpret_cast<const int4*>(&S.idx[i % kGatherDepth][4 * lane]);
+                const uint32_t rowIdx[4] = {static_cast<uint32_t>(rows.x), static_cast<uint32_t>(rows.y),
+                                            static_cast<uint32_t>(rows.z), static_cast<uint32_t>(rows.w)};
 #pragma unroll
-                for (uint32_t j = 0; j < 4; j++) {
-                    const uint32_t rr = 4 * lane + j;
-                    r[j] = static_cast<int32_t>(__ldg(p.perm + ti.start + (rr < ti.count ? rr : 0u)));
+                for (uint32_t r = 0; r < 4; r++) {
+                    const uint32_t tr = 4 * lane + r; // row within the tile
+                    const uint8_t* src = p.desc + uint64_t(rowIdx[r]) * kDims;
+                    uint8_t* dst = S.a[s] + tr * kDims;
+#pragma unroll
+                    for (uint32_t c = 0; c < 8; c++) cpAsync16(dst + ((c ^ (tr & 7u)) << 4), src + (c << 4));
                 }
-                tmaGather4(S.a[s] + lane * 512u, &tmapRow, 0, r[0], r[1], r[2], r[3], &S.aFull[s]);
+                copyIdx(i + kGatherDepth);
+                cpAsyncCommit();
             }
+            issued = i + 1;
             __syncwarp();
         }
-        // Drain: every stage this warp armed must have landed before the CTA can exit.
-        if (lane == 0) {
-            const uint32_t armed = nT < kStages ? nT : kStages;
+        if (gather) {
+            cpAsyncWait<0>();
+            publishUpTo(issued);
+        } else if (lane == 0) {
+            // Drain: every TMA load this warp issued must land before the CTA can exit.
+            const uint32_t armed = issued < kStages ? issued : kStages;
             for (uint32_t s = 0; s < armed; s++) {
-                const uint32_t last = ((nT - 1 - s) / kStages) * kStages + s; // last i with i % kStages == s
-                if (last < nT) mbarWait(&S.aFull[s], (last / kStages) & 1u, abortFlag, nullptr, 12);
+                const uint32_t last = ((issued - 1 - s) / kStages) * kStages + s; // last i with i % kStages == s
+                mbarWait(&S.aFull[s], (last / kStages) & 1u, abortFlag, p.err, 12);
             }
         }
         __syncwarp();
     } else if (nT > 0 && warp == 1) {
         // ------------------------------------------------------------ MMA issuer (one thread)
+        // TMEM: children accumulators in columns [0, 16B) (one buffer), level-2p accumulators in
+        // two 16-column buffers at 256 + 16j.  Order a0 | a1 b0 | a2 b1 | ...: the level-2p MMA of
+        // the next tile runs ahead; the children MMA of tile t waits only for the B warps to have
+        // read tile t-1's children block.  One level: a0 a1 a2 ...
         if (lane == 0) {
             const uint32_t idescA = idescU8(16);
             const uint32_t idescB = idescU8(16 * p.B);
-            uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, slotUses[2] = {0, 0};
-            uint32_t slotOf[2] = {0, 0};  // B slot of tile t, ring indexed by t & 1
+            uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, uses0 = 0, uses1 = 0, slotOf0 = 0, slotOf1 = 0;
             bool ok = true;
-            auto releaseIfLast = [&](uint32_t t) {
-                const uint32_t g = getTile(p, t0 + t).group;
-                const bool last = (t + 1 >= nT) || getTile(p, t0 + t + 1).group != g;
-                if (last) mmaCommit(&S.bEmpty[slotOf[t & 1u]]);
-            };
-            auto issueA = [&](uint32_t t) -> bool {
-                const TileInfo ti = getTile(p, t0 + t);
-                if (ti.group != prevGroup) {
-                    slot ^= 1u;
-                    const uint32_t k = slotUses[slot]++;
-                    if (!mbarWait(&S.bFull[slot], k & 1u, abortFlag, p.err, 20)) return false;
-                    prevGroup = ti.group;
-                }
-                slotOf[t & 1u] = slot;
-                const uint32_t s = t % kStages;
-                if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21)) return false;
-                const uint32_t buf = t & 1u;
-                if (t >= 2) {
-                    uint64_t* freeBar = two ? &S.accBFree[buf] : &S.accAFree[buf];
-                    if (!mbarWait(freeBar, ((t >> 1) - 1u) & 1u, abortFlag, p.err, 22)) return false;
-                }
-                tcFenceAfter();
-                const uint32_t aBase = smemAddr(S.a[s]);
-                const uint32_t bBase = smemAddr(S.b[slot]);
-#pragma unroll
-                for (uint32_t k = 0; k < 4; k++) {
-                    mmaU8(tmem + buf * 256u, smemDescSw128(aBase + 32u * k), smemDescSw128(bBase + 32u * k), idescA,
-                          k > 0 ? 1u : 0u);
-                }
-                mmaCommit(&S.accA[buf]);
+            const uint32_t nSteps = two ? 2 * nT + 1 : nT; // b(nT-1) is step 2nT
+            for (uint32_t k = 0; ok && k < nSteps; k++) {
+                uint32_t t;
+                bool isA;
                 if (!two) {
-                    mmaCommit(&S.aEmpty[s]);
-                    releaseIfLast(t);
+                    t = k;
+                    isA = true;
+                } else if (k == 0) {
+                    t = 0;
+                    isA = true;
+                } else {
+                    // k = 1, 2, 3, ... -> a1 b0 a2 b1 a3 b2 ...
+                    isA = (k & 1u) != 0;
+                    t = isA ? (k + 1u) / 2u : k / 2u - 1u;
+                    if (isA && t >= nT) continue;
                 }
-                return true;
-            };
-            auto issueB = [&](uint32_t t) -> bool {
-                const uint32_t buf = t & 1u;
                 const uint32_t s = t % kStages;
-                if (!mbarWait(&S.accAFree[buf], (t >> 1) & 1u, abortFlag, p.err, 23)) return false;
-                tcFenceAfter();
-                const uint32_t aBase = smemAddr(S.a[s]);
-                const uint32_t bBase = smemAddr(S.b[slotOf[t & 1u]]) + kNodeBytes;
+                const TileInfo ti = tileAtSmem(S, p, t0, t);
+                if (isA) {
+                    const uint32_t j = t & 1u;
+                    if (ti.group != prevGroup) {
+                        slot ^= 1u;
+                        const uint32_t u = slot ? uses1++ : uses0++;
+                        ok = mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 20);
+                        if (!ok) break;
+                        prevGroup = ti.group;
+                    }
+                    if (j) slotOf1 = slot; else slotOf0 = slot;
+                    ok = mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21);
+                    if (ok && t >= 2) ok = mbarWait(&S.accAFree[j], ((t >> 1) - 1u) & 1u, abortFlag, p.err, 22);
+                    if (!ok) break;
+                    tcFenceAfter();
+                    const uint32_t aBase = smemAddr(S.a[s]);
+                    const uint32_t bBase = smemAddr(S.b[slot]);
 #pragma unroll
-                for (uint32_t k = 0; k < 4; k++) {
-                    mmaU8(tmem + buf * 256u, smemDescSw128(aBase + 32u * k), smemDescSw128(bBase + 32u * k), idescB,
-                          k > 0 ? 1u : 0u);
+                    for (uint32_t q4 = 0; q4 < 4; q4++) {
+                        mmaU8(tmem + kTmemA + 16u * j, smemDescSw128(aBase + 32u * q4),
+                              smemDescSw128(bBase + 32u * q4), idescA, q4 > 0 ? 1u : 0u);
+                    }
+                    mmaCommit(&S.accA[j]);
+                    if (!two) {
+                        mmaCommit(&S.aEmpty[s]);
+                        if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[slot]);
+                    }
+                } else {
+                    const uint32_t sl = (t & 1u) ? slotOf1 : slotOf0;
+                    if (t >= 1) ok = mbarWait(&S.accBFree, (t - 1u) & 1u, abortFlag, p.err, 23);
+                    if (!ok) break;
+                    tcFenceAfter();
+                    const uint32_t aBase = smemAddr(S.a[s]);
+                    const uint32_t bBase = smemAddr(S.b[sl]) + kNodeBytes;
+#pragma unroll
+                    for (uint32_t q4 = 0; q4 < 4; q4++) {
+                        mmaU8(tmem, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4), idescB,
+                              q4 > 0 ? 1u : 0u);
+                    }
+                    mmaCommit(&S.accB);
+                    mmaCommit(&S.aEmpty[s]);
+                    if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[sl]);
                 }
-                mmaCommit(&S.accB[buf]);
-                mmaCommit(&S.aEmpty[s]);
-                releaseIfLast(t);
-                return true;
-            };
-            if (two) {
-                // Tensor-core order a0 a1 b0 | b1 a2 | b2 a3 | ... : the next tile's level-2p MMA
-                // runs while the epilogue reads the current tile's children block.
-                ok = issueA(0);
-                if (ok && nT > 1) ok = issueA(1);
-                if (ok) ok = issueB(0);
-                for (uint32_t t = 1; ok && t < nT; t++) {
-                    ok = issueB(t);
-                    if (ok && t + 1 < nT) ok = issueA(t + 1);
-                }
-            } else {
-                for (uint32_t t = 0; ok && t < nT; t++) ok = issueA(t);
             }
             mmaCommit(&S.mmaDone);
-            mbarWait(&S.mmaDone, 0, abortFlag, nullptr, 24);
+            mbarWait(&S.mmaDone, 0, abortFlag, p.err, 24);
         }
         __syncwarp();
-    } else if (nT > 0 && warp >= 2) {
-        // ------------------------------------------------------------ epilogue (128 threads = 128 rows)
+    } else if (nT > 0 && warp >= 2 && warp < 2 + kEpiWarpsPerRole) {
+        // ------------------------------------------------------------ A warps: level-2p argmin
+        // One warp per TMEM lane quarter; each thread owns one tile row.  With two levels the
+        // branch is handed to the B warps through shared memory (written before the arrival
+        // the B warps wait on).
         const uint32_t q = warp & 3u;
         const uint32_t row = q * 32u + lane;
         const uint32_t tRow = tmem + ((q * 32u) << 16);
-        uint32_t bstar0 = 0, bstar1 = 0;
-        auto finalize = [&](const TileInfo& ti, uint32_t node) {
-            if (row < ti.count) {
-                const uint32_t orig = p.perm == nullptr ? ti.start + row : __ldg(p.perm + ti.start + row);
-                if (p.isFinal) {
-                    p.out[orig] = node;
-                } else {
-                    p.nodeNext[orig] = node;
-                    if (smemHist) {
-                        atomicAdd(&S.hist[node], 1u);
-                    } else {
-                        atomicAdd(&p.binCount[node], 1u);
-                    }
-                }
+        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1;
+        for (uint32_t t = 0; t < nT; t++) {
+            const uint32_t j = t & 1u;
+            const TileInfo ti = tileAtSmem(S, p, t0, t);
+            if (ti.group != prevGroup) {
+                slot ^= 1u;
+                prevGroup = ti.group;
             }
-        };
-        auto doA = [&](uint32_t t) -> bool {
-            const uint32_t buf = t & 1u;
-            if (!mbarWait(&S.accA[buf], (t >> 1) & 1u, abortFlag, p.err, 30)) return false;
+            const uint32_t orig = (!two && row < ti.count) ? (gather ? __ldg(p.perm + ti.start + row) : ti.start + row) : 0u;
+            if (!mbarWait(&S.accA[j], (t >> 1) & 1u, abortFlag, p.err, 30)) break;
             tcFenceAfter();
             uint32_t r[16];
-            tmemLoad16(tRow + buf * 256u, r);
+            tmemLoad16(tRow + kTmemA + 16u * j, r);
             tmemWaitTie(r);
+            const uint32_t b = argminScores(r, &S.cn[slot][0][0]);
+            if (two) S.bstar[t % kBsSlots][row] = static_cast<uint8_t>(b);
             tcFenceBefore();
-            mbarArrive(&S.accAFree[buf]);
-            const TileInfo ti = getTile(p, t0 + t);
-            const uint32_t b = argminScores(r, p.cnorm + (p.lbA + ti.group) * kMaxBranch);
-            if (two) {
-                if (buf) bstar1 = b; else bstar0 = b;
-            } else {
-                finalize(ti, ti.group * p.B + b);
+            __syncwarp();
+            if (lane == 0) {
+                mbarArrive(&S.accAFree[j]);
+                if (two) mbarArrive(&S.bsReady[t % kBsSlots]);
             }
-            return true;
-        };
-        auto doB = [&](uint32_t t) -> bool {
-            const uint32_t buf = t & 1u;
-            const uint32_t bs = buf ? bstar1 : bstar0;
-            if (!mbarWait(&S.accB[buf], (t >> 1) & 1u, abortFlag, p.err, 31)) return false;
+            if (!two && row < ti.count) emitRow(S, p, smemHist, orig, ti.group * p.B + b);
+            if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) {
+                __syncwarp();
+                if (lane == 0) mbarArrive(&S.bEmpty[slot]);
+            }
+        }
+    } else if (nT > 0 && two && warp >= 2 + kEpiWarpsPerRole) {
+        // ------------------------------------------------------------ B warps: level-(2p+1) argmin
+        // Each thread reads its row's 16 * B children columns (two 128-column loads), releases the
+        // buffer, and keeps the 16 columns of the child its A warp chose.
+        const uint32_t q = warp & 3u;
+        const uint32_t row = q * 32u + lane;
+        const uint32_t tRow = tmem + ((q * 32u) << 16);
+        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1;
+        for (uint32_t t = 0; t < nT; t++) {
+            const uint32_t j = t & 1u;
+            const TileInfo ti = tileAtSmem(S, p, t0, t);
+            if (ti.group != prevGroup) {
+                slot ^= 1u;
+                prevGroup = ti.group;
+            }
+            const uint32_t orig = row < ti.count ? (gather ? __ldg(p.perm + ti.start + row) : ti.start + row) : 0u;
+            if (!mbarWait(&S.accB, t & 1u, abortFlag, p.err, 31)) break;
+            // acquire the A warps' branch writes for this tile
+            if (!mbarWait(&S.bsReady[t % kBsSlots], (t / kBsSlots) & 1u, abortFlag, p.err, 32)) break;
             tcFenceAfter();
+            const uint32_t bs = S.bstar[t % kBsSlots][row];
             uint32_t sel[16];
 #pragma unroll
             for (int i = 0; i < 16; i++) sel[i] = 0;
-            for (uint32_t k = 0; k < p.B; k += 2) {
-                uint32_t r0[16], r1[16];
-                tmemLoad16(tRow + buf * 256u + 16u * k, r0);
-                if (k + 1 < p.B) tmemLoad16(tRow + buf * 256u + 16u * (k + 1), r1);
-                tmemWaitTie(r0);
-                tieRegs(r1);
+            {
+                uint32_t r[128];
+                tmemLoad128(tRow, r);
+                tmemWaitTie128(r);
+                if (p.B > 8) {
 #pragma unroll
-                for (int i = 0; i < 16; i++) sel[i] = (bs == k) ? r0[i] : sel[i];
-                if (k + 1 < p.B) {
+                    for (uint32_t k = 0; k < 8; k++)
 #pragma unroll
-                    for (int i = 0; i < 16; i++) sel[i] = (bs == k + 1) ? r1[i] : sel[i];
+                        for (int i = 0; i < 16; i++) sel[i] = bs == k ? r[16 * k + i] : sel[i];
+                    tmemLoad128(tRow + 128u, r);
+                    tmemWaitTie128(r);
                 }
+                // the accumulators are in registers: let the next tile's children MMA run
+                tcFenceBefore();
+                __syncwarp();
+                if (lane == 0) mbarArrive(&S.accBFree);
+                const uint32_t k0 = p.B > 8 ? 8u : 0u;
+#pragma unroll
+                for (uint32_t k = 0; k < 8; k++)
+#pragma unroll
+                    for (int i = 0; i < 16; i++) sel[i] = bs == k0 + k ? r[16 * k + i] : sel[i];
             }
-            tcFenceBefore();
-            mbarArrive(&S.accBFree[buf]);
-            const TileInfo ti = getTile(p, t0 + t);
-            const uint64_t child = uint64_t(ti.group) * p.B + bs; // in-level index at level 2p+1
-            const uint32_t b2 = argminScores(sel, p.cnorm + (p.lbB + child) * kMaxBranch);
-            finalize(ti, static_cast<uint32_t>(child * p.B + b2));
-            return true;
-        };
-        bool ok = true;
-        if (two) {
-            ok = doA(0);
-            for (uint32_t t = 0; ok && t < nT; t++) {
-                if (t + 1 < nT) ok = doA(t + 1);
-                if (ok) ok = doB(t);
+            if (row < ti.count) {
+                const uint64_t child = uint64_t(ti.group) * p.B + bs; // in-level index at level 2p+1
+                const uint32_t b2 = argminScores(sel, &S.cn[slot][1 + bs][0]);
+                emitRow(S, p, smemHist, orig, static_cast<uint32_t>(child * p.B + b2));
             }
-        } else {
-            for (uint32_t t = 0; ok && t < nT; t++) ok = doA(t);
+            if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) {
+                __syncwarp();
+                if (lane == 0) mbarArrive(&S.bEmpty[slot]);
+            }
         }
     }
 
@@ -682,6 +802,7 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
     if (n == 0) return 0;
     if (algo == kLookupSimtF32) {
         const uint64_t blocks = (n + kSimtDesc - 1) / kSimtDesc;
+        ScopedKernelTimer timer(kTimedLookupSimt, stream);
         lookupSimtF32<<<static_cast<uint32_t>(blocks), 256, 0, stream>>>(tree.centers, tree.cnorm, tree.B, tree.L, desc,
                                                                          n, leaf);
         RBW_CUDA(cudaGetLastError());
@@ -708,6 +829,7 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
     uint32_t kernels = 0;
     for (uint32_t pass = 0; pass < passes; pass++) {
         PassParams p{};
+        p.desc = desc;
         p.centersSw = tree.centersSw;
         p.cnorm = tree.cnorm;
         p.B = B;
@@ -732,10 +854,14 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
             p.nbBins = nbBins;
             RBW_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t) * nbBins, stream));
         }
-        lookupPassTc<<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, tmapRow, p);
-        RBW_CUDA(cudaGetLastError());
+        {
+            ScopedKernelTimer timer(kTimedLookupPass, stream);
+            lookupPassTc<<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, tmapRow, p);
+            RBW_CUDA(cudaGetLastError());
+        }
         kernels++;
         if (!p.isFinal) {
+            ScopedKernelTimer timer(kTimedRegroup, stream);
             scanBins<<<1, 1024, 0, stream>>>(count, nbBins, rowOff, tileOff, totals);
             RBW_CUDA(cudaGetLastError());
             const uint32_t tileBlocks = std::min<uint32_t>((maxTiles + 255) / 256, 4096);

@@ -98,15 +98,17 @@ __device__ __forceinline__ void mbarArrive(uint64_t* bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
 }
-__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, uint32_t parity)
+// One bounded try: the thread is suspended (not spinning) until the phase completes or the
+// hint (ns) expires, so waiting warps leave the issue slots to the warps doing work.
+__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, uint32_t parity, uint32_t suspendNs = 1000000u)
 {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smemAddr(bar)), "r"(parity)
+        : "r"(smemAddr(bar)), "r"(parity), "r"(suspendNs)
         : "memory");
     return ok != 0;
 }
@@ -121,21 +123,36 @@ __device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t parity, volatil
 {
     if (mbarTryWait(bar, parity)) return true;
     const uint64_t t0 = globalTimerNs();
-    for (uint32_t i = 0;; i++) {
+    for (;;) {
         if (mbarTryWait(bar, parity)) return true;
-        if ((i & 63) == 63) {
-            if (*abortFlag) return false;
-            if (globalTimerNs() - t0 > kWaitLimitNs) {
-                *abortFlag = 1;
-                if (err != nullptr && atomicCAS(&err->code, 0u, 1u) == 0u) {
-                    err->where = site;
-                    err->block = blockIdx.x;
-                    err->detail = parity;
-                }
-                return false;
+        if (*abortFlag) return false;
+        if (globalTimerNs() - t0 > kWaitLimitNs) {
+            *abortFlag = 1;
+            if (err != nullptr && atomicCAS(&err->code, 0u, 1u) == 0u) {
+                err->where = site;
+                err->block = blockIdx.x;
+                err->detail = parity;
             }
+            return false;
         }
     }
+}
+
+// 4-byte asynchronous global -> shared copy (no register dependency) and its group fences.
+__device__ __forceinline__ void cpAsync4(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smemAddr(dst)), "l"(src) : "memory");
+}
+// 16-byte asynchronous global -> shared copy, cached in L2 only.
+__device__ __forceinline__ void cpAsync16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smemAddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // TMA: 2D tiled load and 2D row gather (4 rows per instruction, box one row high).

@@ -32,7 +32,7 @@ def test_lookup_matches_oracle(oracle, B, L, algo):
         assert np.array_equal(got, want), f"n={n}: {np.count_nonzero(got != want)} mismatches"
 
 
-@pytest.mark.parametrize("n", [0, 1, 15, 16, 127, 128, 129, 255, 256, 257, 100003])
+@pytest.mark.parametrize("n", [0, 1, 15, 16, 127, 128, 129, 255, 256, 257, 100003, 2000003])
 def test_lookup_sizes_tensor_vs_simt_vs_oracle(oracle, n):
     B, L = 16, 4
     centers, masks, weights = random_tree(B, L, seed=7)
