@@ -132,6 +132,17 @@ RBW_API int rbw_voc_lookup_scratch_bytes(const rbw_vocabulary* voc, uint64_t nb_
  * Synchronizes the device. */
 RBW_API int rbw_voc_device_errors(const rbw_vocabulary* voc, uint32_t* code, uint32_t* where);
 
+/* No counterpart in the reference.  rbw_voc_lookup for callers that must not allocate device
+ * memory during the call (inside CUDA graph capture, in latency-bound serving loops, under a
+ * fixed memory budget): the same tensor-core lookup, with its working memory taken from one
+ * 8 MiB device array that the library reserves on each GPU for the life of the process.
+ * The first call on a device resolves that array's address and must come before any stream
+ * capture; calls that may overlap on the GPU share the array and race, so serialise them.
+ * Calls needing more than 8 MiB of working memory (about one million descriptors for a
+ * 16-ary, 4-level tree; see rbw_voc_lookup_scratch_bytes) fail with RBW_ERR_INVALID_ARG. */
+RBW_API int rbw_voc_lookup_noalloc(const rbw_vocabulary* voc, const void* dev_desc, uint32_t nb_desc,
+                                   uint32_t* dev_leaf, void* stream);
+
 /* Replaces IVocabulary::~IVocabulary (RapidBoW.cpp:24). */
 RBW_API void rbw_voc_destroy(rbw_vocabulary* voc);
 

@@ -83,6 +83,7 @@ def load_library() -> C.CDLL:
         "rbw_voc_lookup_scratch_bytes": (C.c_int, [vp, u64, C.POINTER(u64)]),
         "rbw_voc_device_errors": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
         "rbw_voc_destroy": (None, [vp]),
+        "rbw_voc_lookup_noalloc": (C.c_int, [vp, vp, u32, vp, vp]),
         "rbw_timing_enable": (None, [i32]),
         "rbw_timing_reset": (C.c_int, []),
         "rbw_timing_read": (C.c_int, [u32, C.POINTER(C.c_double), C.POINTER(u64)]),
@@ -214,6 +215,14 @@ class Vocabulary:
                                            _dev_ptr(out) if n else None, LOOKUP_ALGOS[algo],
                                            _stream_ptr(stream), C.byref(k)))
         self.last_kernels = k.value
+        return out
+
+    def lookup_noalloc(self, desc, out, stream=None):
+        """Lookup whose working memory is the library's fixed per-GPU array (no allocation;
+        see rbw_voc_lookup_noalloc for the limits).  desc: CUDA uint8 [n, 128]; out: CUDA int32 [n]."""
+        n = desc.shape[0]
+        _check(self._lib.rbw_voc_lookup_noalloc(self._h, _dev_ptr(desc) if n else None, n,
+                                                _dev_ptr(out) if n else None, _stream_ptr(stream)))
         return out
 
     def lookup_host(self, desc: np.ndarray, algo: str = "auto") -> np.ndarray:

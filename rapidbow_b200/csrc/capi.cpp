@@ -3,6 +3,7 @@
 #include "rapidbow_b200.h"
 #include "vocabulary.h"
 #include "timing.h"
+#include "capi_internal.h"
 
 #include <cstring>
 #include <new>
@@ -221,3 +222,8 @@ int rbw_timing_read(uint32_t kernel, double* total_ms, uint64_t* launches)
 }
 
 } // extern "C"
+
+namespace rbw {
+const Vocabulary& vocabularyOf(const rbw_vocabulary* h) { return vocOf(h); }
+int runGuarded(const std::function<void()>& f) { return guard(f); }
+} // namespace rbw
