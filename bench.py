@@ -15,6 +15,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -258,12 +259,16 @@ def run_ours(args, world, rank, local):
     hbm_peak, peak_kind = peaks()
     k_avg_ms = k_ms / max(k_n, 1)
     achieved = n * BYTES_PER_DESC / (k_avg_ms / 1e3) / 1e9
+    # DRAM traffic of one pass launch: bytes per descriptor from the ncu capture summarised in
+    # profiles/lookup_pass_tc_2M.md (dram read + write of a 2M-descriptor launch; traffic grows
+    # in proportion to the descriptors), scaled to this launch.
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "lookup_pass_tc_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "lookup_pass_tc_2M.md")
     if os.path.exists(prof):
         with open(prof) as fh:
-            tr = json.load(fh)
-        traffic = tr.get("bytes_per_descriptor") and tr["bytes_per_descriptor"] * n
+            m = re.search(r"^traffic_bytes_per_descriptor:\s*([0-9.]+)", fh.read(), re.M)
+        if m:
+            traffic = float(m.group(1)) * n
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

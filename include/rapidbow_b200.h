@@ -146,6 +146,58 @@ RBW_API int rbw_voc_lookup_noalloc(const rbw_vocabulary* voc, const void* dev_de
 /* Replaces IVocabulary::~IVocabulary (RapidBoW.cpp:24). */
 RBW_API void rbw_voc_destroy(rbw_vocabulary* voc);
 
+/* ------------------------------------------------------------------ inverted file
+ * Replaces rbow::IDataBase (RapidBoW.h:92-107, DataBase.h:35-64, DataBase.cpp:39-197): an
+ * inverted file over the leaf words of a vocabulary, scored with hierarchical tf-idf L1
+ * distances.  The index lives on the GPU and is rebuilt on the device, from all documents,
+ * at the first query after documents were added (the rebuild waits for the device to go
+ * idle).  Documents and queries hold at most 32768 descriptors; max_results at most 1024.
+ * Results are ordered by ascending score, ties by ascending document id (the reference's
+ * std::sort leaves the order of equal scores unspecified). */
+typedef struct rbw_database rbw_database;
+
+/* rbow::createDataBase (RapidBoW.h:107).  The database keeps a non-owning reference to the
+ * vocabulary (DataBase.h:43-45) but copies its weights, so only creation needs it. */
+RBW_API int rbw_db_create(const rbw_vocabulary* voc, rbw_database** out);
+RBW_API void rbw_db_destroy(rbw_database* db);
+
+/* IDataBase::addDoc (RapidBoW.h:98, DataBase.cpp:39-69): host leaf indices of one document.
+ * RBW_ERR_DUPLICATE for an index already present; RBW_ERR_INVALID_ARG for a leaf >= B^L. */
+RBW_API int rbw_db_add(rbw_database* db, uint32_t idx_doc, const uint32_t* host_leaves, uint32_t n);
+
+/* addDoc for many documents: document i owns host_leaves[offsets[i] .. offsets[i+1]).  The
+ * batch is validated first; on failure nothing is added. */
+RBW_API int rbw_db_add_batch(rbw_database* db, const uint32_t* doc_ids, const uint32_t* host_leaves,
+                             const uint64_t* offsets, uint32_t n_docs);
+
+/* IDataBase::query (RapidBoW.h:100-101, DataBase.cpp:71-190): host leaves in; up to
+ * max_results document ids (and their scores, if out_scores is not NULL) out; *n_out results.
+ * Synchronous. */
+RBW_API int rbw_db_query(const rbw_database* db, const uint32_t* host_leaves, uint32_t n, uint32_t max_results,
+                         uint32_t* out_docs, float* out_scores, uint32_t* n_out);
+
+/* IDataBase::queryAndAddDoc (RapidBoW.h:103-104, DataBase.cpp:192-197). */
+RBW_API int rbw_db_query_and_add(rbw_database* db, uint32_t idx_doc, const uint32_t* host_leaves, uint32_t n,
+                                 uint32_t max_results, uint32_t* out_docs, float* out_scores, uint32_t* n_out);
+
+/* Many queries in one launch (no counterpart in the reference, which scores one query per
+ * call): query i owns dev_leaves[dev_offsets[i] .. dev_offsets[i+1]) (device buffers).  Writes
+ * dev_docs / dev_scores [n_queries][max_results] and dev_counts [n_queries], asynchronously on
+ * `stream`; the offsets are read back first (one synchronisation).  Leaves >= B^L are ignored. */
+RBW_API int rbw_db_query_batched(const rbw_database* db, const uint32_t* dev_leaves, const uint64_t* dev_offsets,
+                                 uint32_t n_queries, uint32_t max_results, uint32_t* dev_docs, float* dev_scores,
+                                 uint32_t* dev_counts, void* stream);
+
+/* Number of documents and postings (descriptors) added. */
+RBW_API int rbw_db_info(const rbw_database* db, uint32_t* n_docs, uint64_t* n_postings);
+
+/* The stored reciprocal L1 norm of a document's weight vector (DataBase.cpp:54-68). */
+RBW_API int rbw_db_doc_rcp(const rbw_database* db, uint32_t idx_doc, float* rcp);
+
+/* A leaf's posting list as the reference stores it (DataBase.h:58): document ids ascending,
+ * repeated once per descriptor.  *n = full length; at most `capacity` ids are written. */
+RBW_API int rbw_db_postings(const rbw_database* db, uint32_t leaf, uint32_t* out, uint32_t capacity, uint32_t* n);
+
 /* Optional CUDA-event timing of this library's own kernel launches (no reference
  * counterpart; used by bench.py).  While enabled, each launch of a timed kernel is bracketed by
  * two events on its stream.  rbw_timing_read sums completed launches of one kernel id:

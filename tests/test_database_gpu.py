@@ -1,0 +1,264 @@
+"""Parity of the device-resident inverted file (DataBase.cpp:39-197) against the oracle (reference
+arithmetic and FP64) and against the reference's own DataBase (oracle/_ref), through the C ABI.
+
+Tolerances: postings, document norms and result ids are exact.  Scores: the reference sums
+float terms in double in a fixed order, the kernels sum the same float terms exactly in 64-bit
+fixed point, so a score can differ from the reference-arithmetic oracle by one float ulp when the
+double sum sits next to a float rounding boundary; ranks are then checked through the oracle's
+scores.  Against the FP64 oracle every score is within 1e-6 * max(score, 1) (scores lie in
+[0, 2]; near 0 the bound is absolute).
+"""
+import numpy as np
+import pytest
+
+import rapidbow_b200 as rbw
+from tests.helpers import random_tree
+
+pytestmark = pytest.mark.gpu
+
+
+def _ulp(x):
+    return np.spacing(np.abs(np.float32(x))).astype(np.float64)
+
+
+def make_docs(n_docs, n_leaves, seed, lo=20, hi=600, zipf=0.8):
+    """Documents with log-uniform sizes; leaves drawn from a skewed popularity so some posting
+    lists are long, with repeated leaves inside documents (tf > 1)."""
+    rng = np.random.default_rng(seed)
+    pop = 1.0 / np.arange(1, n_leaves + 1) ** zipf
+    pop = pop[rng.permutation(n_leaves)]
+    pop /= pop.sum()
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), n_docs)).astype(np.int64)
+    docs = []
+    for s in sizes:
+        d = rng.choice(n_leaves, size=s, p=pop).astype(np.uint32)
+        rep = np.nonzero(rng.random(s) < 0.1)[0]
+        rep = rep[rep > 0]
+        d[rep] = d[rep - 1]
+        docs.append(d)
+    return docs
+
+
+def make_queries(docs, n_leaves, n, seed):
+    rng = np.random.default_rng(seed)
+    qs = []
+    for i in range(n):
+        if i % 3 == 2:
+            qs.append(rng.integers(0, n_leaves, size=int(rng.integers(5, 400)), dtype=np.uint32))
+            continue
+        base = docs[int(rng.integers(0, len(docs)))]
+        keep = base[rng.random(base.size) < 0.7]
+        extra = rng.integers(0, n_leaves, size=max(1, base.size // 3), dtype=np.uint32)
+        q = np.concatenate([keep, extra]).astype(np.uint32)
+        qs.append(q[rng.permutation(q.size)])
+    return qs
+
+
+def build_pair(oracle, B, L, docs, ids, seed=0):
+    centers, masks, weights = random_tree(B, L, seed, dup_rate=0.0)
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    db = rbw.DataBase(voc)
+    odb = oracle.db(B, L, weights)
+    for i, d in zip(ids, docs):
+        db.add_doc(int(i), d)
+        odb.add(int(i), d)
+    return voc, db, odb, weights
+
+
+def check_query(db, odb, q, k):
+    docs, scores = db.query(q, k, with_scores=True)
+    odocs, oscores = odb.query(q, k, mode=0)
+    assert docs.size == min(k, odocs.size)
+    if docs.size == 0:
+        return docs, scores
+    oscore = dict(zip(odocs.tolist(), oscores.tolist()))
+    # every returned document is a touched one, with the reference-arithmetic score
+    mine = np.array([oscore[int(d)] for d in docs])
+    assert np.all(np.abs(scores.astype(np.float64) - mine) <= _ulp(mine)), "score differs by more than 1 ulp"
+    assert np.all(np.diff(scores) >= 0)
+    if not np.array_equal(docs, odocs[: docs.size]):
+        # allowed only where the oracle's scores at the differing ranks are within one ulp
+        diff = np.nonzero(docs != odocs[: docs.size])[0]
+        assert np.all(np.abs(mine[diff] - oscores[diff]) <= _ulp(oscores[diff])), "ranking differs"
+    # FP64 oracle: 1e-6 * max(score, 1)
+    fdocs, fscores = odb.query(q, k, mode=1)
+    f = dict(zip(fdocs.tolist(), fscores.tolist()))
+    ref64 = np.array([f[int(d)] for d in docs])
+    assert np.all(np.abs(scores - ref64) <= 1e-6 * np.maximum(ref64, 1.0))
+    return docs, scores
+
+
+@pytest.mark.parametrize("B,L,n_docs", [(16, 2, 120), (16, 3, 400), (10, 4, 300), (16, 4, 600)])
+def test_postings_norms_and_queries(oracle, B, L, n_docs):
+    n_leaves = B ** L
+    docs = make_docs(n_docs, n_leaves, seed=B * 10 + L)
+    rng = np.random.default_rng(7)
+    ids = rng.permutation(np.arange(n_docs, dtype=np.uint32) * 3 + 5)  # sparse, unordered ids
+    _, db, odb, _ = build_pair(oracle, B, L, docs, ids)
+    assert db.info() == (n_docs, sum(d.size for d in docs))
+    # postings are exact (sorted ids with duplicates, as the reference stores them)
+    touched = np.unique(np.concatenate(docs))
+    for leaf in np.concatenate([touched[:: max(1, touched.size // 200)], [0, n_leaves - 1]]):
+        assert np.array_equal(db.postings(int(leaf)), odb.postings(int(leaf)))
+    # norms are bit-exact
+    for i in ids[:50]:
+        assert np.float32(db.doc_rcp(int(i))) == np.float32(odb.doc_rcp(int(i)))
+    for k in (1, 10, 50, 1024):
+        for q in make_queries(docs, n_leaves, 12, seed=k):
+            check_query(db, odb, q, k)
+
+
+def test_self_query_ranks_itself_first(oracle):
+    B, L = 16, 3
+    docs = make_docs(200, B ** L, seed=3)
+    ids = np.arange(200, dtype=np.uint32)
+    _, db, odb, _ = build_pair(oracle, B, L, docs, ids)
+    for i in (0, 17, 199):
+        got, scores = check_query(db, odb, docs[i], 5)
+        # rank 0 is the image itself; its score is not 0 because the skip rule leaves out the
+        # upper levels whose subtrees hold many postings (DataBase.cpp:125)
+        assert got[0] == i and scores[0] < scores[1]
+
+
+def test_matches_reference_database(oracle, reference):
+    """The reference's own DataBase (compiled from its sources) returns the same ranking."""
+    B, L = 16, 3
+    docs = make_docs(500, B ** L, seed=11)
+    ids = np.arange(500, dtype=np.uint32) + 1000
+    _, db, odb, weights = build_pair(oracle, B, L, docs, ids)
+    rdb = reference.db(L, weights)
+    for i, d in zip(ids, docs):
+        rdb.add(int(i), d)
+    for k in (5, 50):
+        for q in make_queries(docs, B ** L, 20, seed=100 + k):
+            got = db.query(q, k)
+            want = rdb.query(q, k)
+            assert got.size == want.size
+            if np.array_equal(got, want):
+                continue
+            # the reference's std::sort leaves equal scores in any order: compare through scores
+            odocs, oscores = odb.query(q, k, mode=0)
+            s = dict(zip(odocs.tolist(), oscores.tolist()))
+            a = np.array([s[int(x)] for x in got])
+            b = np.array([s[int(x)] for x in want])
+            assert np.all(np.abs(a - b) <= _ulp(b))
+
+
+def test_query_and_add_sequence(oracle):
+    """queryAndAddDoc (DataBase.cpp:192-197) in a loop: each query sees exactly the documents
+    added before it, so the index is rebuilt between calls."""
+    B, L = 16, 3
+    docs = make_docs(60, B ** L, seed=5)
+    centers, masks, weights = random_tree(B, L, 1, dup_rate=0.0)
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    db = rbw.DataBase(voc)
+    odb = oracle.db(B, L, weights)
+    for i, d in enumerate(docs):
+        got = db.query_and_add_doc(i, d, 8)
+        odocs, oscores = odb.query(d, 8, mode=0)
+        odb.add(i, d)
+        assert got.size == min(8, odocs.size)
+        if not np.array_equal(got, odocs[: got.size]):
+            s = dict(zip(odocs.tolist(), oscores.tolist()))
+            a = np.array([s[int(x)] for x in got])
+            assert np.all(np.abs(a - oscores[: got.size]) <= _ulp(oscores[: got.size]))
+    assert db.info()[0] == 60
+
+
+def test_batched_equals_single(oracle):
+    import torch
+
+    B, L = 16, 3
+    docs = make_docs(300, B ** L, seed=21)
+    ids = np.arange(300, dtype=np.uint32)
+    _, db, odb, _ = build_pair(oracle, B, L, docs, ids)
+    qs = make_queries(docs, B ** L, 37, seed=9)
+    qs[3] = np.zeros(0, np.uint32)  # empty query: no results
+    k = 20
+    offs = np.zeros(len(qs) + 1, np.int64)
+    offs[1:] = np.cumsum([q.size for q in qs])
+    leaves = torch.from_numpy(np.concatenate(qs).astype(np.int32)).cuda()
+    offsets = torch.from_numpy(offs).cuda()
+    bd, bs, bc = db.query_batched(leaves, offsets, k)
+    torch.cuda.synchronize()
+    bd, bs, bc = bd.cpu().numpy().view(np.uint32), bs.cpu().numpy(), bc.cpu().numpy()
+    assert bc[3] == 0
+    for i, q in enumerate(qs):
+        d, s = db.query(q, k, with_scores=True)
+        assert bc[i] == d.size
+        assert np.array_equal(bd[i, : d.size], d)
+        assert np.array_equal(bs[i, : d.size], s)
+
+
+def test_batched_ignores_out_of_range_leaves(oracle):
+    import torch
+
+    B, L = 16, 2
+    docs = make_docs(50, B ** L, seed=2)
+    _, db, _, _ = build_pair(oracle, B, L, docs, np.arange(50, dtype=np.uint32))
+    q = docs[4][:30]
+    bad = np.concatenate([q, np.array([B ** L, 0xFFFFFFFF, B ** L + 7], np.uint32)])
+    leaves = torch.from_numpy(bad.view(np.int32)).cuda()
+    offsets = torch.tensor([0, bad.size], dtype=torch.int64).cuda()
+    bd, bs, bc = db.query_batched(leaves, offsets, 10)
+    torch.cuda.synchronize()
+    d, s = db.query(q, 10, with_scores=True)
+    assert int(bc[0]) == d.size
+    assert np.array_equal(bd[0, : d.size].cpu().numpy().view(np.uint32), d)
+    assert np.array_equal(bs[0, : d.size].cpu().numpy(), s)
+
+
+def test_many_documents_use_global_accumulators(oracle):
+    """More documents than fit the in-shared-memory accumulators (20480)."""
+    B, L = 16, 3
+    rng = np.random.default_rng(4)
+    n_docs = 25000
+    docs = make_docs(n_docs, B ** L, seed=8, lo=3, hi=40)
+    ids = rng.permutation(n_docs).astype(np.uint32)
+    centers, masks, weights = random_tree(B, L, 2, dup_rate=0.0)
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    db = rbw.DataBase(voc)
+    offs = np.zeros(n_docs + 1, np.uint64)
+    offs[1:] = np.cumsum([d.size for d in docs])
+    db.add_docs(ids, np.concatenate(docs), offs)
+    odb = oracle.db(B, L, weights)
+    for i, d in zip(ids, docs):
+        odb.add(int(i), d)
+    for q in make_queries(docs, B ** L, 8, seed=1):
+        check_query(db, odb, q, 50)
+
+
+def test_edge_cases(oracle):
+    B, L = 16, 2
+    centers, masks, weights = random_tree(B, L, 3, dup_rate=0.0)
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    db = rbw.DataBase(voc)
+    # empty database
+    assert db.query(np.array([1, 2, 3], np.uint32), 10).size == 0
+    db.add_doc(7, np.array([5, 5, 5, 9], np.uint32))
+    db.add_doc(0xFFFFFFF0, np.array([9, 200], np.uint32))
+    db.add_doc(3, np.zeros(0, np.uint32))  # empty document: no postings
+    with pytest.raises(rbw.RbwError) as e:
+        db.add_doc(7, np.array([1], np.uint32))
+    assert e.value.status == rbw.RBW_ERR_DUPLICATE
+    with pytest.raises(rbw.RbwError) as e:
+        db.add_doc(8, np.array([B ** L], np.uint32))
+    assert e.value.status == rbw.RBW_ERR_INVALID_ARG
+    with pytest.raises(rbw.RbwError):
+        db.add_docs(np.array([20, 20], np.uint32), np.array([1, 2], np.uint32), np.array([0, 1, 2], np.uint64))
+    assert db.info() == (3, 6)
+    assert np.array_equal(db.postings(5), [7, 7, 7])
+    assert np.array_equal(db.postings(9), [7, 0xFFFFFFF0])
+    assert db.query(np.array([5], np.uint32), 0).size == 0
+    got = db.query(np.array([9, 5], np.uint32), 10)
+    odb = oracle.db(B, L, weights)
+    odb.add(7, np.array([5, 5, 5, 9], np.uint32))
+    odb.add(0xFFFFFFF0, np.array([9, 200], np.uint32))
+    odb.add(3, np.zeros(0, np.uint32))
+    odocs, _ = odb.query(np.array([9, 5], np.uint32), 10)
+    assert np.array_equal(got, odocs[:10])
+    # adding after a query rebuilds the index
+    db.add_doc(11, np.array([9, 9], np.uint32))
+    assert 11 in db.query(np.array([9, 9], np.uint32), 10).tolist()
+    with pytest.raises(rbw.RbwError):
+        db.query(np.array([5], np.uint32), 2000)
