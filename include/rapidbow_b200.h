@@ -149,9 +149,10 @@ RBW_API void rbw_voc_destroy(rbw_vocabulary* voc);
 /* ------------------------------------------------------------------ inverted file
  * Replaces rbow::IDataBase (RapidBoW.h:92-107, DataBase.h:35-64, DataBase.cpp:39-197): an
  * inverted file over the leaf words of a vocabulary, scored with hierarchical tf-idf L1
- * distances.  The index lives on the GPU and is rebuilt on the device, from all documents,
- * at the first query after documents were added (the rebuild waits for the device to go
- * idle).  Documents and queries hold at most 32768 descriptors; max_results at most 1024.
+ * distances.  The index lives on the GPU.  Adds are staged on the host and indexed on the
+ * device at the next query, in work proportional to the documents added (a delta segment,
+ * merged into the main segment from time to time), ordered with queries by CUDA events.
+ * Documents and queries hold at most 32768 descriptors; max_results at most 1024.
  * Results are ordered by ascending score, ties by ascending document id (the reference's
  * std::sort leaves the order of equal scores unspecified). */
 typedef struct rbw_database rbw_database;
@@ -188,8 +189,21 @@ RBW_API int rbw_db_query_batched(const rbw_database* db, const uint32_t* dev_lea
                                  uint32_t n_queries, uint32_t max_results, uint32_t* dev_docs, float* dev_scores,
                                  uint32_t* dev_counts, void* stream);
 
+/* rbw_db_query_batched with a host copy of the offsets as well, so nothing is read back and the
+ * call does not wait for earlier work on `stream` (for pipelined callers). */
+RBW_API int rbw_db_query_batched_host_offsets(const rbw_database* db, const uint32_t* dev_leaves,
+                                              const uint64_t* dev_offsets, const uint64_t* host_offsets,
+                                              uint32_t n_queries, uint32_t max_results, uint32_t* dev_docs,
+                                              float* dev_scores, uint32_t* dev_counts, void* stream);
+
 /* Number of documents and postings (descriptors) added. */
 RBW_API int rbw_db_info(const rbw_database* db, uint32_t* n_docs, uint64_t* n_postings);
+
+/* Documents in the main and delta segments of the device index, after bringing it up to date
+ * (no counterpart in the reference).  Documents added since the last compaction live in the
+ * delta, which is rebuilt on its own at the next query; the delta is merged into the main
+ * segment once it holds more than max(256, main / 4) documents. */
+RBW_API int rbw_db_segments(const rbw_database* db, uint32_t* main_docs, uint32_t* delta_docs);
 
 /* The stored reciprocal L1 norm of a document's weight vector (DataBase.cpp:54-68). */
 RBW_API int rbw_db_doc_rcp(const rbw_database* db, uint32_t idx_doc, float* rcp);

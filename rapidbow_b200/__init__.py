@@ -110,6 +110,7 @@ def _bind_optional(lib: C.CDLL) -> None:
         "rbw_db_query_and_add": (C.c_int, [vp, u32, vp, u32, u32, vp, vp, C.POINTER(u32)]),
         "rbw_db_query_batched": (C.c_int, [vp, vp, vp, u32, u32, vp, vp, vp, vp]),
         "rbw_db_info": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u64)]),
+        "rbw_db_segments": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
         "rbw_db_doc_rcp": (C.c_int, [vp, u32, C.POINTER(C.c_float)]),
         "rbw_db_postings": (C.c_int, [vp, u32, vp, u32, C.POINTER(u32)]),
     }

@@ -24,8 +24,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
 # Per-file extra flags: the center update must divide exactly like the reference's
 # --use_fast_math kernels.
 EXTRA = {"kmeans_update.cu": ["--use_fast_math"]}
-SOURCES = ["lookup.cu", "kmeans.cu", "kmeans_update.cu", "vocabulary.cu", "scoring.cu", "database.cu", "capi.cpp",
-           "facade.cpp", "timing.cpp", "noalloc.cu"]
+SOURCES = ["lookup.cu", "kmeans.cu", "kmeans_update.cu", "vocabulary.cu", "database.cu", "capi.cpp", "facade.cpp",
+           "timing.cpp", "noalloc.cu"]
 
 
 def _nvcc() -> str:
@@ -77,7 +77,24 @@ def build(verbose: bool = False, force: bool = False) -> str:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_cli(nvcc, verbose)
     return LIB
+
+
+MAKEVOC = os.path.join(LIBDIR, "makevoc")
+
+
+def build_cli(nvcc: str, verbose: bool = False) -> str:
+    """The makevoc command-line tool (csrc/makevoc.cpp), linked against the library."""
+    src = os.path.join(CSRC, "makevoc.cpp")
+    cmd = [nvcc, "-O2", "-std=c++17", "-I", INCLUDE, "-x", "cu", src, "-o", MAKEVOC, "-L", LIBDIR, "-lrapidbow_b200",
+           "-Xlinker", "-rpath,$ORIGIN", *ARCH]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"makevoc build failed:\n{r.stderr}")
+    return MAKEVOC
 
 
 if __name__ == "__main__":

@@ -1,24 +1,35 @@
 // Device-resident inverted file and hierarchical tf-idf scoring (reference: DataBase.cpp:39-197).
 //
-// Index (rebuilt on the device when documents were added since the last query):
-//   * docPrepKernel, one CTA per document: sorts its leaf words in shared memory, computes the
-//     L1 norm of its weight vector over all levels in the reference's order (levels leaf->root,
-//     descriptors in ascending leaf order, double sum; DataBase.cpp:54-68) and run-length
-//     encodes (leaf, tf);
-//   * (slot, tf) pairs are scattered into per-leaf CSR segments.  The pairs of a leaf are the
-//     reference's sorted posting list with repeated document ids folded into tf;
-//   * subtree posting counts of every word (with multiplicity) feed the reference's level skip
-//     rule: a non-leaf word is scored only if its subtree holds < 16 + 4k postings
-//     (DataBase.h:60-61, DataBase.cpp:125).
+// Documents (DataBase.cpp:39-69):
+//   * addDoc only stages the host leaf indices; the device work happens at the next query, for
+//     the documents staged since the last one;
+//   * docPrepKernel, one CTA per new document: sorts its leaf words in shared memory, computes
+//     the L1 norm of its weight vector over all levels in the reference's order (levels
+//     leaf->root, descriptors in ascending leaf order, double sum; DataBase.cpp:54-68) and
+//     run-length encodes it into (leaf, tf) pairs kept per document.
+// Inverted file, in two segments, each a CSR over leaves of (slot, d) pairs, where
+// d = float(tf) * w_leaf * rcp is the document's leaf-level entry (DataBase.cpp:129, the same
+// float products the query would form), plus the raw tf per pair for the upper levels:
+//   * main: documents [0, mainEnd), rebuilt when the newer documents outgrow a fraction of it;
+//   * delta: documents [mainEnd, n), rebuilt from those documents alone after every add, so an
+//     add costs work in proportion to the delta, not to the database.
+//   A leaf's pairs over both segments are the reference's sorted posting list with repeated
+//   document ids folded into tf.  Subtree posting counts of every word (with multiplicity,
+//   both segments) drive the reference's level skip rule: a non-leaf word is scored only if
+//   its subtree holds < 16 + 4k postings (DataBase.h:60-61, DataBase.cpp:125).
 // Queries (any number per launch, uneven sizes):
 //   * queryPrepKernel, one CTA per query: sort, query L1 norm (same order as documents), and
 //     the (level, word, run) entries that survive the skip rule;
 //   * scoreKernel, one CTA per query: warps take entries and add, for every document in the
 //     entry's postings, the reference's term |q - d| - (q + d), q = run*w*qRcp and
-//     d = tf*w*dRcp in float (DataBase.cpp:117,127-131).  Each document's terms are summed in
+//     d = tf*w*dRcp in float (DataBase.cpp:117,127-131; d read from the pair at the leaf
+//     level, formed from the summed tf at upper levels).  Each document's terms are summed in
 //     64-bit fixed point (2^-56 units), so the sum does not depend on the order in which warps
 //     add them; the score is float(sum + 2) (DataBase.cpp:170-174); the k best are chosen by a
 //     radix select on (score, document id).
+// Ordering: index updates run on the database's own stream; a query stream waits for the last
+// update (event), and an update first waits for the queries launched since the previous one,
+// so no host synchronisation is needed between adds and batched queries.
 #include "capi_internal.h"
 #include "kmeans.cuh"
 #include "timing.h"
@@ -36,11 +47,14 @@ namespace {
 
 constexpr uint32_t kMaxDocDesc = 32768;   // descriptors per document or query (in-CTA sort)
 constexpr uint32_t kPrepThreads = 512;
-constexpr uint32_t kScoreThreads = 512;
+constexpr uint32_t kScoreThreads = 1024;
+constexpr uint32_t kSegThreads = 256;
 constexpr uint32_t kSmemDocs = 20480;     // per-document accumulators kept in shared memory
 constexpr uint32_t kMaxK = 1024;
 constexpr double kFixScale = 72057594037927936.0; // 2^56
 constexpr size_t kGlobalAccBudget = size_t(1) << 30; // accumulators of one scoring launch
+constexpr uint32_t kDeltaMinDocs = 256;   // the delta may always hold this many documents
+constexpr uint32_t kDeltaFraction = 4;    // ... or up to main / kDeltaFraction
 
 struct Entry {
     uint32_t level;
@@ -69,6 +83,8 @@ uint32_t nextPow2(uint32_t n)
     while (p < n) p <<= 1;
     return p;
 }
+
+uint32_t blocks(uint64_t n, uint32_t t) { return static_cast<uint32_t>((n + t - 1) / t); }
 
 // Ascending bitonic sort of nPow2 keys in shared memory (all threads of the CTA take part).
 template <typename T>
@@ -112,61 +128,111 @@ __device__ uint32_t loadAndSort(const uint32_t* src, uint32_t n, uint32_t* keys,
     return *nValid;
 }
 
-// Double sum of the weights of every (level, descriptor) in the reference's order.
-__device__ double l1NormSequential(const uint32_t* sorted, uint32_t n, const float* weights, uint32_t B, uint32_t L)
+// Double sum of the weights of every (level, descriptor) in the reference's order (levels
+// leaf->root, descriptors in ascending leaf order).  Warp-collective: the lanes gather 32
+// weights at a time (the next 32 in flight while the current ones are added) and every lane
+// adds them one after another in the same order, so all lanes hold the same sum.
+__device__ double l1NormWarp(const uint32_t* sorted, uint32_t n, const float* weights, uint32_t B, uint32_t L)
 {
+    const uint32_t lane = threadIdx.x & 31u;
     double norm = 0;
     uint64_t span = 1;
     for (uint32_t it = 0; it < L; it++) {
-        const uint32_t level = L - 1 - it;
-        const float* lw = weights + levelBegDev(B, level) * B;
-        for (uint32_t i = 0; i < n; i++) norm += lw[sorted[i] / span];
+        const float* lw = weights + levelBegDev(B, L - 1 - it) * B;
+        float next = lane < n ? lw[sorted[lane] / span] : 0.f;
+        for (uint32_t base = 0; base < n; base += 32) {
+            const float cur = next;
+            const uint32_t ahead = base + 32 + lane;
+            next = ahead < n ? lw[sorted[ahead] / span] : 0.f;
+            if (n - base >= 32) {
+#pragma unroll
+                for (uint32_t j = 0; j < 32; j++) norm += __shfl_sync(0xFFFFFFFFu, cur, j);
+            } else {
+                for (uint32_t j = 0; j < n - base; j++) norm += __shfl_sync(0xFFFFFFFFu, cur, j);
+            }
+        }
         span *= B;
     }
     return norm;
 }
 
-// ------------------------------------------------------------------ index build
-__global__ void __launch_bounds__(kPrepThreads) docPrepKernel(const uint32_t* leaves, const uint64_t* off,
-                                                              const float* weights, uint32_t B, uint32_t L,
-                                                              uint64_t nbLeaves, float* rcpF, uint64_t* pairTmp,
-                                                              uint32_t* pairCount, uint32_t* leafPairCnt,
-                                                              unsigned long long* leafPostCnt)
+// ------------------------------------------------------------------ documents
+// One CTA per new document (slot s0 + blockIdx.x).  newLeaves holds the new documents' leaves
+// back to back, starting at posting offset docOff[s0].
+__global__ void __launch_bounds__(kPrepThreads) docPrepKernel(const uint32_t* newLeaves, const uint64_t* docOff,
+                                                              uint32_t s0, const float* weights, uint32_t B,
+                                                              uint32_t L, uint64_t nbLeaves, float* rcpF,
+                                                              uint64_t* docPairs, uint32_t* pairCount)
 {
     extern __shared__ uint32_t keys[];
     __shared__ uint32_t cnt, nValid;
-    const uint32_t doc = blockIdx.x;
-    const uint64_t beg = off[doc];
+    const uint32_t slot = s0 + blockIdx.x;
+    const uint64_t beg = docOff[slot];
     if (threadIdx.x == 0) cnt = 0;
-    const uint32_t n = loadAndSort(leaves + beg, static_cast<uint32_t>(off[doc + 1] - beg), keys, nbLeaves, &nValid);
-    if (threadIdx.x == 0) rcpF[doc] = float(1 / l1NormSequential(keys, n, weights, B, L)); // DataBase.cpp:68
+    const uint32_t n = loadAndSort(newLeaves + (beg - docOff[s0]), static_cast<uint32_t>(docOff[slot + 1] - beg),
+                                   keys, nbLeaves, &nValid);
+    if (threadIdx.x < 32) {
+        const double norm = l1NormWarp(keys, n, weights, B, L);
+        if (threadIdx.x == 0) rcpF[slot] = float(1 / norm); // DataBase.cpp:68
+    }
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint32_t k = keys[i];
         if (i == 0 || keys[i - 1] != k) {
             uint32_t run = 1;
             while (i + run < n && keys[i + run] == k) run++;
-            const uint32_t p = atomicAdd(&cnt, 1u);
-            pairTmp[beg + p] = (uint64_t(k) << 32) | run;
-            atomicAdd(&leafPairCnt[k], 1u);
-            atomicAdd(&leafPostCnt[k], static_cast<unsigned long long>(run));
+            docPairs[beg + atomicAdd(&cnt, 1u)] = (uint64_t(k) << 32) | run;
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0) pairCount[doc] = cnt;
+    if (threadIdx.x == 0) pairCount[slot] = cnt;
 }
 
-__global__ void scatterPairsKernel(const uint64_t* off, const uint64_t* pairTmp, const uint32_t* pairCount,
-                                   const uint32_t* leafOff, uint32_t* cursor, uint64_t* pairs)
+// Per-leaf pair and posting counts of the documents [s0, s0 + gridDim.x).
+__global__ void segCountKernel(const uint64_t* docOff, const uint64_t* docPairs, const uint32_t* pairCount,
+                               uint32_t s0, uint32_t* leafPairCnt, unsigned long long* leafPost)
 {
-    const uint32_t doc = blockIdx.x;
-    const uint64_t beg = off[doc];
-    for (uint32_t p = threadIdx.x; p < pairCount[doc]; p += blockDim.x) {
-        const uint64_t v = pairTmp[beg + p];
+    const uint32_t slot = s0 + blockIdx.x;
+    const uint64_t beg = docOff[slot];
+    for (uint32_t p = threadIdx.x; p < pairCount[slot]; p += blockDim.x) {
+        const uint64_t v = docPairs[beg + p];
+        const uint32_t leaf = static_cast<uint32_t>(v >> 32);
+        atomicAdd(&leafPairCnt[leaf], 1u);
+        atomicAdd(&leafPost[leaf], static_cast<unsigned long long>(static_cast<uint32_t>(v)));
+    }
+}
+
+// Scatters the documents' pairs into the segment: pairs[] = slot << 32 | bits of the leaf-level
+// document entry d = tf * w_leaf * rcp (DataBase.cpp:129, the same float products as at query
+// time), tf[] = the raw count for the virtual inverted files of upper levels.
+__global__ void segScatterKernel(const uint64_t* docOff, const uint64_t* docPairs, const uint32_t* pairCount,
+                                 uint32_t s0, const float* leafWeights, const float* rcpF, const uint32_t* leafOff,
+                                 uint32_t* cursor, uint64_t* pairs, uint32_t* tfs)
+{
+    const uint32_t slot = s0 + blockIdx.x;
+    const uint64_t beg = docOff[slot];
+    const float rcp = rcpF[slot];
+    for (uint32_t p = threadIdx.x; p < pairCount[slot]; p += blockDim.x) {
+        const uint64_t v = docPairs[beg + p];
         const uint32_t leaf = static_cast<uint32_t>(v >> 32);
         const uint32_t tf = static_cast<uint32_t>(v);
+        const float d = float(tf) * leafWeights[leaf] * rcp;
         const uint32_t pos = leafOff[leaf] + atomicAdd(&cursor[leaf], 1u);
-        pairs[pos] = (uint64_t(doc) << 32) | tf;
+        pairs[pos] = (uint64_t(slot) << 32) | __float_as_uint(d);
+        tfs[pos] = tf;
     }
+}
+
+__global__ void leafOffTail(const uint32_t* leafPairCnt, uint32_t* leafOff, uint64_t nLeaves)
+{
+    leafOff[nLeaves] = leafOff[nLeaves - 1] + leafPairCnt[nLeaves - 1];
+}
+
+// Leaf-level word counts = main + delta postings per leaf.
+__global__ void leafPostCombine(const unsigned long long* mainPost, const unsigned long long* deltaPost,
+                                unsigned long long* out, uint64_t n)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = mainPost[i] + (deltaPost ? deltaPost[i] : 0ull);
 }
 
 // Postings under each word of `level`, from the counts of the level below (bottom-up).
@@ -179,11 +245,6 @@ __global__ void wordPostKernel(unsigned long long* wordPost, uint32_t B, uint32_
     unsigned long long s = 0;
     for (uint32_t c = 0; c < B; c++) s += below[c];
     wordPost[levelBegDev(B, level) * B + w] = s;
-}
-
-__global__ void leafOffTail(const uint32_t* leafPairCnt, uint32_t* leafOff, uint64_t nLeaves)
-{
-    leafOff[nLeaves] = leafOff[nLeaves - 1] + leafPairCnt[nLeaves - 1];
 }
 
 // ------------------------------------------------------------------ queries
@@ -200,7 +261,10 @@ __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* 
     Entry* out = entries + (beg - qOff[0]) * L;
     if (threadIdx.x == 0) cnt = 0;
     const uint32_t n = loadAndSort(qLeaves + beg, static_cast<uint32_t>(qOff[q + 1] - beg), keys, nbLeaves, &nValid);
-    if (threadIdx.x == 0) qRcpF[q] = float(1 / l1NormSequential(keys, n, weights, B, L)); // DataBase.cpp:77-94
+    if (threadIdx.x < 32) {
+        const double norm = l1NormWarp(keys, n, weights, B, L);
+        if (threadIdx.x == 0) qRcpF[q] = float(1 / norm); // DataBase.cpp:77-94
+    }
     uint64_t span = 1;
     const uint64_t limit = 16ull + 4ull * k; // DataBase.h:60-61, DataBase.cpp:125
     for (uint32_t it = 0; it < L; it++) {
@@ -224,14 +288,19 @@ __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* 
     if (threadIdx.x == 0) entryCount[q] = cnt;
 }
 
+struct SegmentView {
+    const uint32_t* leafOff;   // [nbLeaves + 1]
+    const uint64_t* pairs;     // slot << 32 | float bits of the leaf-level document entry
+    const uint32_t* tf;        // descriptors of the document under the leaf
+};
+
 struct ScoreParams {
     const Entry* entries;
     const uint32_t* entryCount;
     const uint64_t* qOff;
     const float* qRcpF;
     const float* weights;
-    const uint32_t* leafOff;
-    const uint64_t* pairs;
+    SegmentView seg[2];        // main, delta
     const float* rcpF;
     const uint32_t* slotDoc;
     uint32_t nDocs;
@@ -240,7 +309,7 @@ struct ScoreParams {
     uint32_t k;
     uint32_t qBase;             // first query of this launch
     unsigned long long* gAcc;   // [launch queries][nDocs] when the accumulators do not fit shared memory
-    uint32_t* gBits;            // [launch queries][(nDocs + 31) / 32]
+    uint8_t* gTouched;          // [launch queries][nDocs]
     uint32_t* outDocs;          // [nq][k]
     float* outScores;           // [nq][k]
     uint32_t* outCount;         // [nq]
@@ -248,11 +317,11 @@ struct ScoreParams {
 
 __device__ __forceinline__ float termOf(float q, float d) { return fabsf(q - d) - (q + d); }
 
-__device__ __forceinline__ void addTerm(unsigned long long* acc, uint32_t* bits, uint32_t slot, float term)
+__device__ __forceinline__ void addTerm(unsigned long long* acc, uint8_t* touched, uint32_t slot, float term)
 {
     const long long fx = llrint(static_cast<double>(term) * kFixScale);
     atomicAdd(&acc[slot], static_cast<unsigned long long>(fx));
-    atomicOr(&bits[slot >> 5], 1u << (slot & 31u));
+    touched[slot] = 1; // every writer stores the same value
 }
 
 // Float bits mapped so that unsigned order is numeric order (negative scores included).
@@ -275,12 +344,13 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
     __shared__ unsigned long long sel[kMaxK];
     const uint32_t local = blockIdx.x;
     const uint32_t q = P.qBase + local;
-    const uint32_t nWords = (P.nDocs + 31) / 32;
     const bool inSmem = P.gAcc == nullptr;
     unsigned long long* acc = inSmem ? dyn : P.gAcc + uint64_t(local) * P.nDocs;
-    uint32_t* bits = inSmem ? reinterpret_cast<uint32_t*>(dyn + P.nDocs) : P.gBits + uint64_t(local) * nWords;
-    for (uint32_t i = threadIdx.x; i < P.nDocs; i += blockDim.x) acc[i] = 0;
-    for (uint32_t i = threadIdx.x; i < nWords; i += blockDim.x) bits[i] = 0;
+    uint8_t* touched = inSmem ? reinterpret_cast<uint8_t*>(dyn + P.nDocs) : P.gTouched + uint64_t(local) * P.nDocs;
+    for (uint32_t i = threadIdx.x; i < P.nDocs; i += blockDim.x) {
+        acc[i] = 0;
+        touched[i] = 0;
+    }
     if (threadIdx.x == 0) nTouched = 0;
     __syncthreads();
 
@@ -292,32 +362,46 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
         const Entry en = ent[e];
         const float w = P.weights[en.widx];
         const float qv = float(en.run) * w * qRcp;
-        if (en.level == P.L - 1) {
-            const uint32_t a = P.leafOff[en.word], b = P.leafOff[en.word + 1];
-            for (uint32_t p = a + lane; p < b; p += 32) {
-                const uint64_t pr = P.pairs[p];
-                const uint32_t slot = static_cast<uint32_t>(pr >> 32);
-                const float d = float(static_cast<uint32_t>(pr)) * w * P.rcpF[slot];
-                addTerm(acc, bits, slot, termOf(qv, d));
-            }
-        } else {
-            // Virtual inverted file of a non-leaf word: the union of the leaf lists below it,
-            // counted per document (DataBase.cpp:150-164).  The skip rule keeps it short, so
-            // each lane scans it for the documents it owns.
-            const uint64_t span = ipowDev(P.B, P.L - 1 - en.level);
-            const uint32_t a = P.leafOff[uint64_t(en.word) * span], b = P.leafOff[(uint64_t(en.word) + 1) * span];
-            for (uint32_t p = a + lane; p < b; p += 32) {
-                const uint32_t slot = static_cast<uint32_t>(P.pairs[p] >> 32);
-                bool first = true;
-                for (uint32_t r = a; r < p && first; r++) first = static_cast<uint32_t>(P.pairs[r] >> 32) != slot;
-                if (!first) continue;
-                uint32_t tf = 0;
-                for (uint32_t r = p; r < b; r++) {
-                    const uint64_t v = P.pairs[r];
-                    if (static_cast<uint32_t>(v >> 32) == slot) tf += static_cast<uint32_t>(v);
+        const bool leafLevel = en.level == P.L - 1;
+        const uint64_t span = ipowDev(P.B, P.L - 1 - en.level);
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const uint64_t* pairs = P.seg[s].pairs;
+            const uint32_t a = P.seg[s].leafOff[uint64_t(en.word) * span];
+            const uint32_t b = P.seg[s].leafOff[(uint64_t(en.word) + 1) * span];
+            if (leafLevel) {
+                // four pairs per lane in flight
+                uint32_t p = a + lane;
+                for (; p + 96 < b; p += 128) {
+                    uint64_t pr[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) pr[u] = pairs[p + 32 * u];
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+                        addTerm(acc, touched, static_cast<uint32_t>(pr[u] >> 32),
+                                termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
                 }
-                const float d = float(tf) * w * P.rcpF[slot];
-                addTerm(acc, bits, slot, termOf(qv, d));
+                for (; p < b; p += 32) {
+                    const uint64_t pr = pairs[p];
+                    addTerm(acc, touched, static_cast<uint32_t>(pr >> 32),
+                            termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
+                }
+            } else {
+                // Virtual inverted file of a non-leaf word: the union of the leaf lists below
+                // it, counted per document (DataBase.cpp:150-164).  A document lives in one
+                // segment only, and the skip rule keeps the union short, so each lane scans the
+                // segment's range for the documents whose first pair it holds.
+                for (uint32_t p = a + lane; p < b; p += 32) {
+                    const uint32_t slot = static_cast<uint32_t>(pairs[p] >> 32);
+                    bool first = true;
+                    for (uint32_t r = a; r < p && first; r++) first = static_cast<uint32_t>(pairs[r] >> 32) != slot;
+                    if (!first) continue;
+                    uint32_t tf = 0;
+                    for (uint32_t r = p; r < b; r++)
+                        if (static_cast<uint32_t>(pairs[r] >> 32) == slot) tf += P.seg[s].tf[r];
+                    const float d = float(tf) * w * P.rcpF[slot];
+                    addTerm(acc, touched, slot, termOf(qv, d));
+                }
             }
         }
     }
@@ -328,7 +412,7 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
     uint32_t myTouched = 0;
     for (uint32_t i = threadIdx.x; i < P.nDocs; i += blockDim.x) {
         unsigned long long key = ~0ull;
-        if (bits[i >> 5] & (1u << (i & 31u))) {
+        if (touched[i]) {
             const double sum = static_cast<double>(static_cast<long long>(acc[i])) / kFixScale;
             const float score = float(sum + 2.0f);
             key = (static_cast<unsigned long long>(orderedBits(score)) << 32) | P.slotDoc[i];
@@ -390,7 +474,46 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
     if (threadIdx.x == 0) P.outCount[q] = want;
 }
 
-uint32_t blocks(uint64_t n, uint32_t t) { return static_cast<uint32_t>((n + t - 1) / t); }
+// Device memory from the library's stream-ordered pool, grown on a stream (keeping a prefix).
+class PoolBuffer
+{
+public:
+    PoolBuffer() = default;
+    PoolBuffer(const PoolBuffer&) = delete;
+    PoolBuffer& operator=(const PoolBuffer&) = delete;
+    template <typename T>
+    T* as() const { return static_cast<T*>(mPtr); }
+    void* get() const { return mPtr; }
+    // Ensures capacity >= need bytes; the first `keep` bytes survive a reallocation.
+    void reserve(size_t need, size_t keep, cudaStream_t s)
+    {
+        if (need <= mCap) return;
+        const size_t cap = std::max(need, mCap + mCap / 2);
+        void* p = nullptr;
+        RBW_CUDA(cudaMallocFromPoolAsync(&p, cap, libraryPool(), s));
+        if (keep && mPtr) RBW_CUDA(cudaMemcpyAsync(p, mPtr, keep, cudaMemcpyDeviceToDevice, s));
+        if (mPtr) RBW_CUDA(cudaFreeAsync(mPtr, s));
+        mPtr = p;
+        mCap = cap;
+    }
+    void release(cudaStream_t s)
+    {
+        if (mPtr) cudaFreeAsync(mPtr, s);
+        mPtr = nullptr;
+        mCap = 0;
+    }
+
+private:
+    void* mPtr = nullptr;
+    size_t mCap = 0;
+};
+
+struct Segment {
+    PoolBuffer leafOff;   // u32 [nbLeaves + 1]
+    PoolBuffer pairs;     // u64 slot << 32 | float bits of the leaf-level document entry
+    PoolBuffer tf;        // u32 per pair
+    uint32_t slotBeg = 0, slotEnd = 0;
+};
 
 } // namespace
 
@@ -398,25 +521,49 @@ uint32_t blocks(uint64_t n, uint32_t t) { return static_cast<uint32_t>((n + t - 
 class DataBase
 {
 public:
-    explicit DataBase(const Vocabulary& v) : mVoc{v}, mB{v.branch()}, mL{v.levels()}
+    explicit DataBase(const Vocabulary& v) : mB{v.branch()}, mL{v.levels()}
     {
         mNbLeaves = ipowDev(mB, mL);
         mNbWords = levelBeg(mB, mL) * mB;
+        if (mNbLeaves >= 0xFFFFFFFFull) throw Error(kUnsupported, "tree too large for a DataBase");
         mWeights.reset(mNbWords * 4);
         RBW_CUDA(cudaMemcpy(mWeights.get(), v.weights().data(), mNbWords * 4, cudaMemcpyHostToDevice));
-        mHostOff.push_back(0);
+        mHostDocOff.push_back(0);
         RBW_CUDA(cudaStreamCreateWithFlags(&mStream, cudaStreamNonBlocking));
+        RBW_CUDA(cudaEventCreateWithFlags(&mIndexReady, cudaEventDisableTiming));
+        // empty index: zero offsets in both segments, zero word counts
+        for (Segment* sg : {&mMain, &mDelta}) {
+            sg->leafOff.reserve((mNbLeaves + 1) * 4, 0, mStream);
+            sg->pairs.reserve(8, 0, mStream);
+            sg->tf.reserve(4, 0, mStream);
+            RBW_CUDA(cudaMemsetAsync(sg->leafOff.get(), 0, (mNbLeaves + 1) * 4, mStream));
+        }
+        mMainLeafPost.reserve(mNbLeaves * 8, 0, mStream);
+        RBW_CUDA(cudaMemsetAsync(mMainLeafPost.get(), 0, mNbLeaves * 8, mStream));
+        mWordPost.reserve(mNbWords * 8, 0, mStream);
+        RBW_CUDA(cudaMemsetAsync(mWordPost.get(), 0, mNbWords * 8, mStream));
+        for (PoolBuffer* b : {&mDocOff, &mDocPairs, &mPairCount, &mRcpF, &mSlotDoc}) b->reserve(64, 0, mStream);
+        RBW_CUDA(cudaMemsetAsync(mDocOff.get(), 0, 8, mStream));
+        RBW_CUDA(cudaEventRecord(mIndexReady, mStream));
+        RBW_CUDA(cudaStreamSynchronize(mStream));
     }
     ~DataBase()
     {
-        if (mStream) cudaStreamDestroy(mStream);
+        waitQueriesOnStream();
+        for (PoolBuffer* b : {&mDocOff, &mDocPairs, &mPairCount, &mRcpF, &mSlotDoc, &mMainLeafPost, &mWordPost,
+                              &mMain.leafOff, &mMain.pairs, &mMain.tf, &mDelta.leafOff, &mDelta.pairs, &mDelta.tf})
+            b->release(mStream);
+        cudaStreamSynchronize(mStream);
+        for (auto& kv : mQueryEvents) cudaEventDestroy(kv.second);
+        cudaEventDestroy(mIndexReady);
+        cudaStreamDestroy(mStream);
     }
 
     void addDoc(uint32_t id, const uint32_t* leaves, uint32_t n)
     {
         std::unique_lock<std::shared_mutex> lk(mMu);
         checkDoc(id, leaves, n);
-        appendLocked(id, leaves, n);
+        stageLocked(id, leaves, n);
     }
     void addDocs(const uint32_t* ids, const uint32_t* leaves, const uint64_t* off, uint32_t nDocs)
     {
@@ -430,7 +577,7 @@ public:
             if (!seen.emplace(ids[d], d).second) throw Error(kDuplicate, "Duplicate document index");
         }
         for (uint32_t d = 0; d < nDocs; d++)
-            appendLocked(ids[d], leaves + off[d], static_cast<uint32_t>(off[d + 1] - off[d]));
+            stageLocked(ids[d], leaves + off[d], static_cast<uint32_t>(off[d + 1] - off[d]));
     }
 
     // Host leaves in, host results out (the reference's query).  Synchronous.
@@ -442,45 +589,41 @@ public:
             if (leaves[i] >= mNbLeaves) throw Error(kInvalidArg, "leaf index out of range");
         if (k == 0) return 0;
         const uint64_t off[2] = {0, n};
-        cudaMemPool_t pool = libraryPool();
-        const size_t inBytes = 16 + size_t(n) * 4;
-        const size_t outBytes = size_t(k) * 8 + 16;
+        cudaStream_t s = mStream;
         void* din = nullptr;
         void* dout = nullptr;
-        RBW_CUDA(cudaMallocFromPoolAsync(&din, inBytes, pool, mStream));
-        RBW_CUDA(cudaMallocFromPoolAsync(&dout, outBytes, pool, mStream));
+        RBW_CUDA(cudaMallocFromPoolAsync(&din, 16 + size_t(n) * 4, libraryPool(), s));
+        RBW_CUDA(cudaMallocFromPoolAsync(&dout, size_t(k) * 8 + 16, libraryPool(), s));
         uint32_t got = 0;
         try {
             uint64_t* dOff = static_cast<uint64_t*>(din);
             uint32_t* dLeaves = reinterpret_cast<uint32_t*>(dOff + 2);
-            RBW_CUDA(cudaMemcpyAsync(dOff, off, 16, cudaMemcpyHostToDevice, mStream));
-            if (n) RBW_CUDA(cudaMemcpyAsync(dLeaves, leaves, size_t(n) * 4, cudaMemcpyHostToDevice, mStream));
+            RBW_CUDA(cudaMemcpyAsync(dOff, off, 16, cudaMemcpyHostToDevice, s));
+            if (n) RBW_CUDA(cudaMemcpyAsync(dLeaves, leaves, size_t(n) * 4, cudaMemcpyHostToDevice, s));
             uint32_t* dDocs = static_cast<uint32_t*>(dout);
             float* dScores = reinterpret_cast<float*>(dDocs + k);
             uint32_t* dCount = reinterpret_cast<uint32_t*>(dScores + k);
-            queryBatched(dLeaves, dOff, 1, k, dDocs, dScores, dCount, mStream, off);
-            RBW_CUDA(cudaMemcpyAsync(&got, dCount, 4, cudaMemcpyDeviceToHost, mStream));
-            RBW_CUDA(cudaStreamSynchronize(mStream));
+            queryBatched(dLeaves, dOff, 1, k, dDocs, dScores, dCount, s, off);
+            RBW_CUDA(cudaMemcpyAsync(&got, dCount, 4, cudaMemcpyDeviceToHost, s));
+            RBW_CUDA(cudaStreamSynchronize(s));
             if (got) {
-                RBW_CUDA(cudaMemcpyAsync(docs, dDocs, size_t(got) * 4, cudaMemcpyDeviceToHost, mStream));
-                if (scores)
-                    RBW_CUDA(cudaMemcpyAsync(scores, dScores, size_t(got) * 4, cudaMemcpyDeviceToHost, mStream));
+                RBW_CUDA(cudaMemcpyAsync(docs, dDocs, size_t(got) * 4, cudaMemcpyDeviceToHost, s));
+                if (scores) RBW_CUDA(cudaMemcpyAsync(scores, dScores, size_t(got) * 4, cudaMemcpyDeviceToHost, s));
             }
         } catch (...) {
-            cudaFreeAsync(din, mStream);
-            cudaFreeAsync(dout, mStream);
-            cudaStreamSynchronize(mStream);
+            cudaFreeAsync(din, s);
+            cudaFreeAsync(dout, s);
+            cudaStreamSynchronize(s);
             throw;
         }
-        RBW_CUDA(cudaFreeAsync(din, mStream));
-        RBW_CUDA(cudaFreeAsync(dout, mStream));
-        RBW_CUDA(cudaStreamSynchronize(mStream));
+        RBW_CUDA(cudaFreeAsync(din, s));
+        RBW_CUDA(cudaFreeAsync(dout, s));
+        RBW_CUDA(cudaStreamSynchronize(s));
         return got;
     }
 
     // Device leaves and offsets in, device results out; the kernels run asynchronously on
-    // `stream`.  The index is first brought up to date (synchronously) if documents were added.
-    // hostOff, if given, is a host copy of dOff (saves reading the offsets back).
+    // `stream`.  hostOff, if given, is a host copy of dOff (saves reading the offsets back).
     void queryBatched(const uint32_t* dLeaves, const uint64_t* dOff, uint32_t nq, uint32_t k, uint32_t* dDocs,
                       float* dScores, uint32_t* dCount, cudaStream_t stream, const uint64_t* hostOff = nullptr)
     {
@@ -503,16 +646,17 @@ public:
         }
         if (maxN && dLeaves == nullptr) throw Error(kInvalidArg, "null argument");
         const uint64_t totalLeaves = hostOff[nq] - hostOff[0];
-        ensureIndex();
+        updateIndex();
         std::shared_lock<std::shared_mutex> lk(mMu);
+        RBW_CUDA(cudaStreamWaitEvent(stream, mIndexReady, 0));
         if (k == 0) {
             RBW_CUDA(cudaMemsetAsync(dCount, 0, size_t(nq) * 4, stream));
             return;
         }
+        const uint32_t nDocs = mIndexed;
         cudaMemPool_t pool = libraryPool();
-        const uint32_t nWords = (mNbDocs + 31) / 32;
-        const bool smemAcc = mNbDocs <= kSmemDocs;
-        const size_t perQueryAcc = size_t(mNbDocs) * 8 + size_t(nWords) * 4;
+        const bool smemAcc = nDocs <= kSmemDocs;
+        const size_t perQueryAcc = size_t(nDocs) * 9;
         const uint32_t chunk =
             smemAcc ? nq : static_cast<uint32_t>(std::clamp<size_t>(kGlobalAccBudget / perQueryAcc, 1, nq));
         const size_t entBytes = std::max<uint64_t>(totalLeaves, 1) * mL * sizeof(Entry);
@@ -536,11 +680,12 @@ public:
             P.qOff = dOff;
             P.qRcpF = static_cast<const float*>(qr);
             P.weights = mWeights.as<float>();
-            P.leafOff = mLeafOff.as<uint32_t>();
-            P.pairs = mPairs.as<uint64_t>();
+            P.seg[0] = SegmentView{mMain.leafOff.as<uint32_t>(), mMain.pairs.as<uint64_t>(), mMain.tf.as<uint32_t>()};
+            P.seg[1] = SegmentView{mDelta.leafOff.as<uint32_t>(), mDelta.pairs.as<uint64_t>(),
+                                   mDelta.tf.as<uint32_t>()};
             P.rcpF = mRcpF.as<float>();
             P.slotDoc = mSlotDoc.as<uint32_t>();
-            P.nDocs = mNbDocs;
+            P.nDocs = nDocs;
             P.B = mB;
             P.L = mL;
             P.k = k;
@@ -549,10 +694,10 @@ public:
             P.outCount = dCount;
             size_t smem = 0;
             if (smemAcc) {
-                smem = size_t(mNbDocs) * 8 + size_t(nWords) * 4;
+                smem = size_t(nDocs) * 9;
             } else {
                 P.gAcc = static_cast<unsigned long long*>(acc);
-                P.gBits = reinterpret_cast<uint32_t*>(P.gAcc + size_t(chunk) * mNbDocs);
+                P.gTouched = reinterpret_cast<uint8_t*>(P.gAcc + size_t(chunk) * nDocs);
             }
             RBW_CUDA(cudaFuncSetAttribute(scoreKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
             for (uint32_t q0 = 0; q0 < nq; q0 += chunk) {
@@ -565,6 +710,7 @@ public:
         RBW_CUDA(cudaFreeAsync(cnt, stream));
         RBW_CUDA(cudaFreeAsync(qr, stream));
         RBW_CUDA(cudaFreeAsync(acc, stream));
+        recordQuery(stream);
     }
 
     uint32_t nbDocs()
@@ -575,17 +721,26 @@ public:
     uint64_t nbPostings()
     {
         std::shared_lock<std::shared_mutex> lk(mMu);
-        return mHostLeaves.size();
+        return mHostDocOff.back();
+    }
+    // Documents in the main and delta segments of the current index (diagnostics).
+    void segments(uint32_t* mainDocs, uint32_t* deltaDocs)
+    {
+        updateIndex();
+        std::shared_lock<std::shared_mutex> lk(mMu);
+        if (mainDocs) *mainDocs = mMain.slotEnd - mMain.slotBeg;
+        if (deltaDocs) *deltaDocs = mDelta.slotEnd - mDelta.slotBeg;
     }
 
     float docRcp(uint32_t id)
     {
-        ensureIndex();
+        updateIndex();
         std::shared_lock<std::shared_mutex> lk(mMu);
         const auto it = mSlotOf.find(id);
         if (it == mSlotOf.end()) throw Error(kInvalidArg, "unknown document");
         float v = 0;
-        RBW_CUDA(cudaMemcpy(&v, mRcpF.as<float>() + it->second, 4, cudaMemcpyDeviceToHost));
+        RBW_CUDA(cudaMemcpyAsync(&v, mRcpF.as<float>() + it->second, 4, cudaMemcpyDeviceToHost, mStream));
+        RBW_CUDA(cudaStreamSynchronize(mStream));
         return v;
     }
 
@@ -594,15 +749,29 @@ public:
     std::vector<uint32_t> postings(uint32_t leaf)
     {
         if (leaf >= mNbLeaves) throw Error(kInvalidArg, "leaf out of range");
-        ensureIndex();
+        updateIndex();
         std::shared_lock<std::shared_mutex> lk(mMu);
-        uint32_t ab[2] = {0, 0};
-        RBW_CUDA(cudaMemcpy(ab, mLeafOff.as<uint32_t>() + leaf, 8, cudaMemcpyDeviceToHost));
-        std::vector<uint64_t> pr(ab[1] - ab[0]);
-        if (!pr.empty())
-            RBW_CUDA(cudaMemcpy(pr.data(), mPairs.as<uint64_t>() + ab[0], pr.size() * 8, cudaMemcpyDeviceToHost));
         std::vector<uint32_t> out;
-        for (const uint64_t v : pr) out.insert(out.end(), static_cast<uint32_t>(v), mHostIds[v >> 32]);
+        for (const Segment* sg : {&mMain, &mDelta}) {
+            uint32_t ab[2] = {0, 0};
+            RBW_CUDA(cudaMemcpyAsync(ab, sg->leafOff.as<uint32_t>() + leaf, 8, cudaMemcpyDeviceToHost, mStream));
+            RBW_CUDA(cudaStreamSynchronize(mStream));
+            if (ab[1] < ab[0]) throw Error(kInternal, "inconsistent posting offsets");
+            std::vector<uint64_t> pr(ab[1] - ab[0]);
+            std::vector<uint32_t> tf(pr.size());
+            if (!pr.empty()) {
+                RBW_CUDA(cudaMemcpyAsync(pr.data(), sg->pairs.as<uint64_t>() + ab[0], pr.size() * 8,
+                                         cudaMemcpyDeviceToHost, mStream));
+                RBW_CUDA(cudaMemcpyAsync(tf.data(), sg->tf.as<uint32_t>() + ab[0], tf.size() * 4,
+                                         cudaMemcpyDeviceToHost, mStream));
+                RBW_CUDA(cudaStreamSynchronize(mStream));
+            }
+            for (size_t i = 0; i < pr.size(); i++) {
+                if (tf[i] > kMaxDocDesc || (pr[i] >> 32) >= mHostIds.size())
+                    throw Error(kInternal, "inconsistent posting entry");
+                out.insert(out.end(), tf[i], mHostIds[pr[i] >> 32]);
+            }
+        }
         std::sort(out.begin(), out.end());
         return out;
     }
@@ -617,94 +786,154 @@ private:
             if (leaves[i] >= mNbLeaves) throw Error(kInvalidArg, "leaf index out of range");
     }
 
-    void appendLocked(uint32_t id, const uint32_t* leaves, uint32_t n)
+    void stageLocked(uint32_t id, const uint32_t* leaves, uint32_t n)
     {
         mSlotOf.emplace(id, static_cast<uint32_t>(mHostIds.size()));
         mHostIds.push_back(id);
-        mHostLeaves.insert(mHostLeaves.end(), leaves, leaves + n);
-        mHostOff.push_back(mHostLeaves.size());
-        mMaxDocN = std::max(mMaxDocN, n);
-        mDirty = true;
+        mStage.insert(mStage.end(), leaves, leaves + n);
+        mHostDocOff.push_back(mHostDocOff.back() + n);
+        mStageMaxN = std::max(mStageMaxN, n);
     }
 
-    // Rebuilds the device index from all documents.  A rebuild replaces buffers that earlier
-    // query launches may still read, so it first waits for the device to go idle.
-    void ensureIndex()
+    // Makes the stream wait for every query launched since the last index update.
+    void waitQueriesOnStream()
+    {
+        std::lock_guard<std::mutex> lk(mEvMu);
+        for (auto& kv : mQueryEvents) RBW_CUDA(cudaStreamWaitEvent(mStream, kv.second, 0));
+    }
+
+    void recordQuery(cudaStream_t stream)
+    {
+        std::lock_guard<std::mutex> lk(mEvMu);
+        auto it = mQueryEvents.find(stream);
+        if (it == mQueryEvents.end()) {
+            cudaEvent_t ev = nullptr;
+            RBW_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            it = mQueryEvents.emplace(stream, ev).first;
+        }
+        RBW_CUDA(cudaEventRecord(it->second, stream));
+    }
+
+    // CSR of the documents [s0, s1) into `sg`; their per-leaf posting counts into leafPost.
+    void buildSegment(Segment& sg, uint32_t s0, uint32_t s1, unsigned long long* leafPost)
+    {
+        const uint64_t pairsUpper = mHostDocOff[s1] - mHostDocOff[s0];
+        if (pairsUpper >= 0xFFFFFFFFull) throw Error(kUnsupported, "more than 2^32 postings in one segment");
+        sg.slotBeg = s0;
+        sg.slotEnd = s1;
+        sg.pairs.reserve(std::max<uint64_t>(pairsUpper, 1) * 8, 0, mStream);
+        sg.tf.reserve(std::max<uint64_t>(pairsUpper, 1) * 4, 0, mStream);
+        void* tmp = nullptr;
+        const size_t cntBytes = mNbLeaves * 4;
+        const size_t scanBytes = scanTempWords(mNbLeaves) * 4;
+        RBW_CUDA(cudaMallocFromPoolAsync(&tmp, 2 * cntBytes + scanBytes, libraryPool(), mStream));
+        uint32_t* leafPairCnt = static_cast<uint32_t*>(tmp);
+        uint32_t* cursor = leafPairCnt + mNbLeaves;
+        uint32_t* scanTmp = cursor + mNbLeaves;
+        RBW_CUDA(cudaMemsetAsync(leafPairCnt, 0, 2 * cntBytes, mStream));
+        RBW_CUDA(cudaMemsetAsync(leafPost, 0, mNbLeaves * 8, mStream));
+        if (s1 > s0) {
+            segCountKernel<<<s1 - s0, kSegThreads, 0, mStream>>>(mDocOff.as<uint64_t>(), mDocPairs.as<uint64_t>(),
+                                                                mPairCount.as<uint32_t>(), s0, leafPairCnt, leafPost);
+            RBW_CUDA(cudaGetLastError());
+        }
+        uint32_t* leafOff = sg.leafOff.as<uint32_t>();
+        exclusiveScanU32(leafPairCnt, leafOff, mNbLeaves, scanTmp, mStream);
+        leafOffTail<<<1, 1, 0, mStream>>>(leafPairCnt, leafOff, mNbLeaves);
+        if (s1 > s0) {
+            segScatterKernel<<<s1 - s0, kSegThreads, 0, mStream>>>(
+                mDocOff.as<uint64_t>(), mDocPairs.as<uint64_t>(), mPairCount.as<uint32_t>(), s0,
+                mWeights.as<float>() + levelBeg(mB, mL - 1) * mB, mRcpF.as<float>(), leafOff, cursor,
+                sg.pairs.as<uint64_t>(), sg.tf.as<uint32_t>());
+        }
+        RBW_CUDA(cudaGetLastError());
+        RBW_CUDA(cudaFreeAsync(tmp, mStream));
+    }
+
+    // Brings the device index up to date with the staged documents.  Enqueues work on the
+    // database stream only; queries order themselves after it through mIndexReady.
+    void updateIndex()
     {
         {
             std::shared_lock<std::shared_mutex> lk(mMu);
-            if (!mDirty) return;
+            if (mIndexed == mHostIds.size()) return;
         }
         std::unique_lock<std::shared_mutex> lk(mMu);
-        if (!mDirty) return;
-        if (mBuilt) RBW_CUDA(cudaDeviceSynchronize());
-        const uint32_t nd = static_cast<uint32_t>(mHostIds.size());
-        const uint64_t nl = mHostLeaves.size();
-        if (nl > 0xFFFFFFFFull) throw Error(kUnsupported, "more than 2^32 postings");
-        mNbDocs = nd;
-        mSlotDoc.reset(std::max<uint64_t>(nd, 1) * 4);
-        mRcpF.reset(std::max<uint64_t>(nd, 1) * 4);
-        mLeafOff.reset((mNbLeaves + 1) * 4);
-        mPairs.reset(std::max<uint64_t>(nl, 1) * 8);
-        mWordPost.reset(mNbWords * 8);
-        DeviceBuffer dLeaves(std::max<uint64_t>(nl, 1) * 4), dOff((uint64_t(nd) + 1) * 8);
-        DeviceBuffer pairTmp(std::max<uint64_t>(nl, 1) * 8), pairCount(std::max<uint64_t>(nd, 1) * 4);
-        DeviceBuffer leafPairCnt(mNbLeaves * 4), cursor(mNbLeaves * 4);
-        DeviceBuffer scanTmp(scanTempWords(mNbLeaves) * 4);
-        unsigned long long* leafPostCnt = mWordPost.as<unsigned long long>() + levelBeg(mB, mL - 1) * mB;
-        {
-            ScopedKernelTimer timer(kTimedIndex, mStream);
-            if (nl)
-                RBW_CUDA(cudaMemcpyAsync(dLeaves.get(), mHostLeaves.data(), nl * 4, cudaMemcpyHostToDevice, mStream));
-            RBW_CUDA(cudaMemcpyAsync(dOff.get(), mHostOff.data(), (uint64_t(nd) + 1) * 8, cudaMemcpyHostToDevice,
+        const uint32_t s0 = mIndexed;
+        const uint32_t s1 = static_cast<uint32_t>(mHostIds.size());
+        if (s0 == s1) return;
+        ScopedKernelTimer timer(kTimedIndex, mStream);
+        waitQueriesOnStream();
+        const uint64_t p0 = mHostDocOff[s0], p1 = mHostDocOff[s1];
+        // 1. per-document arrays, grown in place
+        mDocOff.reserve((uint64_t(s1) + 1) * 8, (uint64_t(s0) + 1) * 8, mStream);
+        mDocPairs.reserve(std::max<uint64_t>(p1, 1) * 8, p0 * 8, mStream);
+        mPairCount.reserve(uint64_t(s1) * 4, uint64_t(s0) * 4, mStream);
+        mRcpF.reserve(uint64_t(s1) * 4, uint64_t(s0) * 4, mStream);
+        mSlotDoc.reserve(uint64_t(s1) * 4, uint64_t(s0) * 4, mStream);
+        RBW_CUDA(cudaMemcpyAsync(mDocOff.as<uint64_t>() + s0 + 1, mHostDocOff.data() + s0 + 1,
+                                 uint64_t(s1 - s0) * 8, cudaMemcpyHostToDevice, mStream));
+        RBW_CUDA(cudaMemcpyAsync(mSlotDoc.as<uint32_t>() + s0, mHostIds.data() + s0, uint64_t(s1 - s0) * 4,
+                                 cudaMemcpyHostToDevice, mStream));
+        void* newLeaves = nullptr;
+        RBW_CUDA(cudaMallocFromPoolAsync(&newLeaves, std::max<uint64_t>(p1 - p0, 1) * 4, libraryPool(), mStream));
+        if (p1 > p0)
+            RBW_CUDA(cudaMemcpyAsync(newLeaves, mStage.data(), (p1 - p0) * 4, cudaMemcpyHostToDevice, mStream));
+        const size_t smem = size_t(nextPow2(std::max(mStageMaxN, 1u))) * 4;
+        RBW_CUDA(cudaFuncSetAttribute(docPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        docPrepKernel<<<s1 - s0, kPrepThreads, smem, mStream>>>(
+            static_cast<const uint32_t*>(newLeaves), mDocOff.as<uint64_t>(), s0, mWeights.as<float>(), mB, mL,
+            mNbLeaves, mRcpF.as<float>(), mDocPairs.as<uint64_t>(), mPairCount.as<uint32_t>());
+        RBW_CUDA(cudaGetLastError());
+        RBW_CUDA(cudaFreeAsync(newLeaves, mStream));
+        mStage.clear();
+        mStageMaxN = 0;
+
+        // 2. segments: compact everything into main when the delta outgrows its share
+        unsigned long long* leafWords = mWordPost.as<unsigned long long>() + levelBeg(mB, mL - 1) * mB;
+        const uint32_t mainEnd = mMain.slotEnd;
+        if (s1 - mainEnd > std::max(kDeltaMinDocs, mainEnd / kDeltaFraction)) {
+            buildSegment(mMain, 0, s1, mMainLeafPost.as<unsigned long long>());
+            buildSegment(mDelta, s1, s1, leafWords);
+            RBW_CUDA(cudaMemcpyAsync(leafWords, mMainLeafPost.get(), mNbLeaves * 8, cudaMemcpyDeviceToDevice,
                                      mStream));
-            if (nd)
-                RBW_CUDA(cudaMemcpyAsync(mSlotDoc.get(), mHostIds.data(), uint64_t(nd) * 4, cudaMemcpyHostToDevice,
-                                         mStream));
-            RBW_CUDA(cudaMemsetAsync(leafPairCnt.get(), 0, leafPairCnt.bytes(), mStream));
-            RBW_CUDA(cudaMemsetAsync(mWordPost.get(), 0, mWordPost.bytes(), mStream));
-            RBW_CUDA(cudaMemsetAsync(cursor.get(), 0, cursor.bytes(), mStream));
-            if (nd) {
-                const size_t smem = size_t(nextPow2(std::max(mMaxDocN, 1u))) * 4;
-                RBW_CUDA(cudaFuncSetAttribute(docPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-                docPrepKernel<<<nd, kPrepThreads, smem, mStream>>>(
-                    dLeaves.as<uint32_t>(), dOff.as<uint64_t>(), mWeights.as<float>(), mB, mL, mNbLeaves,
-                    mRcpF.as<float>(), pairTmp.as<uint64_t>(), pairCount.as<uint32_t>(), leafPairCnt.as<uint32_t>(),
-                    leafPostCnt);
-                RBW_CUDA(cudaGetLastError());
-            }
-            exclusiveScanU32(leafPairCnt.as<uint32_t>(), mLeafOff.as<uint32_t>(), mNbLeaves, scanTmp.as<uint32_t>(),
-                             mStream);
-            leafOffTail<<<1, 1, 0, mStream>>>(leafPairCnt.as<uint32_t>(), mLeafOff.as<uint32_t>(), mNbLeaves);
-            if (nd) {
-                scatterPairsKernel<<<nd, 256, 0, mStream>>>(dOff.as<uint64_t>(), pairTmp.as<uint64_t>(),
-                                                            pairCount.as<uint32_t>(), mLeafOff.as<uint32_t>(),
-                                                            cursor.as<uint32_t>(), mPairs.as<uint64_t>());
-            }
-            for (uint32_t level = mL - 1; level-- > 0;) {
-                wordPostKernel<<<blocks(ipowDev(mB, level + 1), 256), 256, 0, mStream>>>(
-                    mWordPost.as<unsigned long long>(), mB, level);
-            }
-            RBW_CUDA(cudaGetLastError());
+        } else {
+            void* deltaPost = nullptr;
+            RBW_CUDA(cudaMallocFromPoolAsync(&deltaPost, mNbLeaves * 8, libraryPool(), mStream));
+            buildSegment(mDelta, mainEnd, s1, static_cast<unsigned long long*>(deltaPost));
+            leafPostCombine<<<blocks(mNbLeaves, 256), 256, 0, mStream>>>(
+                mMainLeafPost.as<unsigned long long>(), static_cast<unsigned long long*>(deltaPost), leafWords,
+                mNbLeaves);
+            RBW_CUDA(cudaFreeAsync(deltaPost, mStream));
         }
-        RBW_CUDA(cudaStreamSynchronize(mStream));
-        mDirty = false;
-        mBuilt = true;
+        // 3. subtree posting counts of the upper levels
+        for (uint32_t level = mL - 1; level-- > 0;) {
+            wordPostKernel<<<blocks(ipowDev(mB, level + 1), 256), 256, 0, mStream>>>(
+                mWordPost.as<unsigned long long>(), mB, level);
+        }
+        RBW_CUDA(cudaGetLastError());
+        RBW_CUDA(cudaEventRecord(mIndexReady, mStream));
+        mIndexed = s1;
     }
 
-    const Vocabulary& mVoc;
     uint32_t mB, mL;
     uint64_t mNbLeaves = 0, mNbWords = 0;
-    DeviceBuffer mWeights, mWordPost;
-    std::vector<uint32_t> mHostIds, mHostLeaves;
-    std::vector<uint64_t> mHostOff;
+    DeviceBuffer mWeights;
+    // host state
+    std::vector<uint32_t> mHostIds;        // slot -> document id
+    std::vector<uint64_t> mHostDocOff;     // slot -> first posting (prefix sums of sizes)
     std::unordered_map<uint32_t, uint32_t> mSlotOf;
-    uint32_t mMaxDocN = 0;
-    bool mDirty = true;
-    bool mBuilt = false;
-    uint32_t mNbDocs = 0;
-    DeviceBuffer mSlotDoc, mRcpF, mLeafOff, mPairs;
+    std::vector<uint32_t> mStage;          // leaves of documents [mIndexed, nSlots)
+    uint32_t mStageMaxN = 0;
+    uint32_t mIndexed = 0;                 // documents in the device index
+    // device state (library pool, ordered on mStream)
+    PoolBuffer mDocOff, mDocPairs, mPairCount, mRcpF, mSlotDoc;
+    Segment mMain, mDelta;
+    PoolBuffer mMainLeafPost, mWordPost;
     cudaStream_t mStream = nullptr;
+    cudaEvent_t mIndexReady = nullptr;
+    std::unordered_map<cudaStream_t, cudaEvent_t> mQueryEvents;
+    std::mutex mEvMu;
     std::shared_mutex mMu;
 };
 
@@ -781,6 +1010,17 @@ int rbw_db_query_batched(const rbw_database* db, const uint32_t* dev_leaves, con
     });
 }
 
+int rbw_db_query_batched_host_offsets(const rbw_database* db, const uint32_t* dev_leaves, const uint64_t* dev_offsets,
+                                      const uint64_t* host_offsets, uint32_t n_queries, uint32_t max_results,
+                                      uint32_t* dev_docs, float* dev_scores, uint32_t* dev_counts, void* stream)
+{
+    return rbw::runGuarded([&] {
+        if (host_offsets == nullptr) throw rbw::Error(rbw::kInvalidArg, "null host offsets");
+        dbOf(db).queryBatched(dev_leaves, dev_offsets, n_queries, max_results, dev_docs, dev_scores, dev_counts,
+                              static_cast<cudaStream_t>(stream), host_offsets);
+    });
+}
+
 int rbw_db_info(const rbw_database* db, uint32_t* n_docs, uint64_t* n_postings)
 {
     return rbw::runGuarded([&] {
@@ -788,6 +1028,11 @@ int rbw_db_info(const rbw_database* db, uint32_t* n_docs, uint64_t* n_postings)
         if (n_docs) *n_docs = d.nbDocs();
         if (n_postings) *n_postings = d.nbPostings();
     });
+}
+
+int rbw_db_segments(const rbw_database* db, uint32_t* main_docs, uint32_t* delta_docs)
+{
+    return rbw::runGuarded([&] { dbOf(db).segments(main_docs, delta_docs); });
 }
 
 int rbw_db_doc_rcp(const rbw_database* db, uint32_t idx_doc, float* rcp)

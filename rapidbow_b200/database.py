@@ -81,6 +81,12 @@ class DataBase:
         _check(self._lib.rbw_db_info(self._h, C.byref(nd), C.byref(npost)))
         return nd.value, npost.value
 
+    def segments(self) -> Tuple[int, int]:
+        """Documents in the (main, delta) segments of the device index, after an update."""
+        m, d = C.c_uint32(), C.c_uint32()
+        _check(self._lib.rbw_db_segments(self._h, C.byref(m), C.byref(d)))
+        return m.value, d.value
+
     def doc_rcp(self, doc: int) -> float:
         v = C.c_float()
         _check(self._lib.rbw_db_doc_rcp(self._h, doc, C.byref(v)))

@@ -262,3 +262,75 @@ def test_edge_cases(oracle):
     assert 11 in db.query(np.array([9, 9], np.uint32), 10).tolist()
     with pytest.raises(rbw.RbwError):
         db.query(np.array([5], np.uint32), 2000)
+
+
+def test_incremental_segments_match_oracle(oracle):
+    """Adds after queries go to the delta segment, which is merged into the main segment once it
+    outgrows max(256, main / 4) documents; results match the oracle at every step."""
+    B, L = 16, 3
+    docs = make_docs(900, B ** L, seed=31, lo=10, hi=200)
+    centers, masks, weights = random_tree(B, L, 6, dup_rate=0.0)
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    db = rbw.DataBase(voc)
+    odb = oracle.db(B, L, weights)
+    qs = make_queries(docs, B ** L, 6, seed=4)
+
+    def add(lo, hi):
+        for i in range(lo, hi):
+            db.add_doc(i, docs[i])
+            odb.add(i, docs[i])
+
+    add(0, 300)
+    for q in qs:
+        check_query(db, odb, q, 20)
+    assert db.segments() == (300, 0)       # 300 > 256: first update builds the main segment
+    add(300, 310)
+    for q in qs:
+        check_query(db, odb, q, 20)
+    assert db.segments() == (300, 10)      # small delta
+    for i in range(310, 330):              # query-and-add loop: one document per update
+        got = db.query_and_add_doc(i, docs[i], 5)
+        od, _ = odb.query(docs[i], 5)
+        odb.add(i, docs[i])
+        assert got.size == min(5, od.size)
+    assert db.segments()[0] == 300
+    add(330, 620)                           # delta 320 > max(256, 75): merged
+    check_query(db, odb, qs[0], 50)
+    assert db.segments() == (620, 0)
+    leaf = int(docs[5][0])
+    assert np.array_equal(db.postings(leaf), odb.postings(leaf))
+    add(620, 900)
+    for q in qs:
+        check_query(db, odb, q, 1024)
+    for i in (0, 450, 899):
+        assert np.float32(db.doc_rcp(i)) == np.float32(odb.doc_rcp(i))
+
+
+def test_batched_queries_interleaved_with_adds(oracle):
+    """Batched queries on a user stream and adds on the host thread need no synchronisation:
+    each batch sees the documents added before it was issued."""
+    import torch
+
+    B, L = 16, 2
+    docs = make_docs(120, B ** L, seed=12, lo=5, hi=80)
+    centers, masks, weights = random_tree(B, L, 9, dup_rate=0.0)
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    db = rbw.DataBase(voc)
+    odb = oracle.db(B, L, weights)
+    q = docs[3][:40]
+    leaves = torch.from_numpy(q.astype(np.int32)).cuda()
+    offsets = torch.tensor([0, q.size], dtype=torch.int64).cuda()
+    stream = torch.cuda.Stream()
+    outs = []
+    for step in range(4):
+        for i in range(step * 30, step * 30 + 30):
+            db.add_doc(i, docs[i])
+            odb.add(i, docs[i])
+        with torch.cuda.stream(stream):
+            outs.append(db.query_batched(leaves, offsets, 10, stream=stream))
+        want, _ = odb.query(q, 10)
+        outs[-1] = (outs[-1], want[:10].copy())
+    torch.cuda.synchronize()
+    for (d, s, c), want in outs:
+        assert int(c[0]) == want.size
+        assert set(d[0, : want.size].cpu().numpy().view(np.uint32).tolist()) == set(want.tolist())
