@@ -47,6 +47,11 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-scoring", action="store_true", help="skip the inverted-file scoring workload")
     p.add_argument("--db-docs", type=int, default=20000, help="images in the scoring database")
+    p.add_argument("--serving", action="store_true",
+                   help="also run the serving workload (1M-word tree, 100,000 images, Poisson arrivals)")
+    p.add_argument("--serving-docs", type=int, default=100_000)
+    p.add_argument("--serving-rate", type=float, default=2000.0, help="arrivals per second")
+    p.add_argument("--serving-seconds", type=float, default=10.0)
     return p.parse_args()
 
 
@@ -138,12 +143,14 @@ def barrier(world):
 
 
 def allreduce_max(world, x: float) -> float:
+    """Max over ranks (timings are reported as the slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -315,10 +322,13 @@ def run_ours(args, world, rank, local):
         v, sn, dt = cpu_baseline(threads, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{sn} descriptors through a B=16 L=4 tree in {dt:.1f} s"}
-    if not args.no_scoring:
+    if not args.no_scoring or args.serving:
         del desc, out, ref32
         torch.cuda.empty_cache()
+    if not args.no_scoring:
         line["scoring"] = scoring_bench(args, voc, dev, world, rank)
+    if args.serving:
+        line["serving"] = serving_bench(args, dev, rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -443,6 +453,98 @@ def scoring_bench(args, voc, dev, world, rank):
             voc, ids, doc_leaves, offs, queries, k, docs.cpu().numpy().view(np.uint32), counts.cpu().numpy(),
             args.cpu_seconds)
     return res
+
+
+SERVING_WORKLOAD = ("serving: 1M-word tree (B=10, L=6) trained on 10M SIFT-like descriptors from a 4,096-component "
+                    "mixture with Zipf(1.1) weights (k-means++ init, 10 Lloyd iterations); device-resident database of "
+                    "100,000 images of log-uniform 300-8,000 descriptors; query images of log-uniform 300-8,000 "
+                    "descriptors arrive as a Poisson stream; lookup + scoring, top-100, continuous batching")
+
+
+def serving_bench(args, dev, rank):
+    """Build (B=10, L=6) timed, then a Poisson request stream through rapidbow_b200.Server.
+    Database images are drawn from the leaf distribution of 8M looked-up descriptors (the
+    posting-list shape of real lookups without generating 234M descriptors); query images are
+    slices of a pool of fresh descriptors and go through the server's lookup."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    import rapidbow_b200 as rbw
+    from rapidbow_b200.synth import sift_like
+
+    rng = np.random.default_rng(77 + rank)
+    train = sift_like(10_000_000, seed=2, n_components=4096, zipf=1.1, device=dev)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    voc = rbw.build_vocabulary(train, 10, nb_doc=args.serving_docs, nb_levels=6, init="kmeans++", seed=11,
+                               max_iterations=10)
+    torch.cuda.synchronize(dev)
+    build_s = time.perf_counter() - t0
+    del train
+    pool = sift_like(8_000_000, seed=3, n_components=4096, zipf=1.1, device=dev)
+    leaf_pool = voc.lookup(pool).cpu().numpy().view(np.uint32)
+    del pool
+    sizes = np.exp(rng.uniform(np.log(300), np.log(8000), args.serving_docs)).astype(np.int64)
+    doc_leaves = leaf_pool[rng.integers(0, leaf_pool.size, int(sizes.sum()))]
+    offs = np.zeros(args.serving_docs + 1, np.uint64)
+    offs[1:] = np.cumsum(sizes)
+    db = rbw.DataBase(voc)
+    db.add_docs(np.arange(args.serving_docs, dtype=np.uint32), doc_leaves, offs)
+    del doc_leaves
+    qpool = sift_like(4_000_000, seed=4, n_components=4096, zipf=1.1, device=dev).cpu().numpy()
+    torch.cuda.empty_cache()
+    srv = rbw.Server(voc, db, max_results=100)
+    # warm-up (also builds the index)
+    for _ in range(3):
+        srv.wait(srv.submit(qpool[:2000]))
+    srv.reset_stats()
+
+    n_req = int(args.serving_rate * args.serving_seconds)
+    gaps = rng.exponential(1.0 / args.serving_rate, n_req)
+    qs = np.exp(rng.uniform(np.log(300), np.log(8000), n_req)).astype(np.int64)
+    starts = rng.integers(0, qpool.shape[0] - 8000, n_req)
+    ids = [0] * n_req
+
+    def collector():
+        for i in range(n_req):
+            while ids[i] == 0:
+                time.sleep(0.0001)
+            srv.wait(ids[i])
+
+    col = threading.Thread(target=collector)
+    rbw.timing_reset()
+    rbw.timing_enable(True)
+    col.start()
+    t_begin = time.perf_counter()
+    t_next = t_begin
+    for i in range(n_req):
+        t_next += gaps[i]
+        ahead = t_next - time.perf_counter()
+        if ahead > 0.001:
+            time.sleep(ahead - 0.0005)
+        while time.perf_counter() < t_next:
+            pass
+        ids[i] = srv.submit(qpool[starts[i]: starts[i] + qs[i]])
+    col.join()
+    elapsed = time.perf_counter() - t_begin
+    torch.cuda.synchronize(dev)
+    rbw.timing_enable(False)
+    kernels = {}
+    for name in ("lookup_pass_tc", "lookup_regroup", "score"):
+        ms, n = rbw.timing_read(name)
+        kernels[name] = {"launches": n, "total_ms": ms, "mean_ms": ms / max(n, 1)}
+    st = srv.stats()
+    srv.close()
+    return {"workload": SERVING_WORKLOAD, "build_s": build_s, "requests": n_req,
+            "offered_rate_qps": args.serving_rate, "value": n_req / elapsed, "unit": "queries/s",
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+            "mean_batch_requests": st["mean_batch_requests"], "batches": st["batches"],
+            "max_inflight_batches_seen": st["max_inflight_seen"], "descriptors_per_request_mean": float(qs.mean()),
+            "db_postings": int(sizes.sum()), "gpu_event_ms_by_kernel": kernels,
+            "note": "latency = submit to result on the host, including the host-to-device copy of the descriptors; "
+                    "kernel times are event spans on streams that share the GPU"}
 
 
 def scoring_cpu_baseline(voc, ids, doc_leaves, offs, queries, k, got_docs, got_counts, seconds):

@@ -133,8 +133,8 @@ RBW_API int rbw_voc_lookup_scratch_bytes(const rbw_vocabulary* voc, uint64_t nb_
 RBW_API int rbw_voc_device_errors(const rbw_vocabulary* voc, uint32_t* code, uint32_t* where);
 
 /* No counterpart in the reference.  rbw_voc_lookup for callers that must not allocate device
- * memory during the call (inside CUDA graph capture, in latency-bound serving loops, under a
- * fixed memory budget): the same tensor-core lookup, with its working memory taken from one
+ * memory during the call (latency-bound serving loops, plug-ins inside an application that owns
+ * the GPU memory, fixed memory budgets): the same tensor-core lookup, with its working memory taken from one
  * 8 MiB device array that the library reserves on each GPU for the life of the process.
  * The first call on a device resolves that array's address and must come before any stream
  * capture; calls that may overlap on the GPU share the array and race, so serialise them.
@@ -211,6 +211,50 @@ RBW_API int rbw_db_doc_rcp(const rbw_database* db, uint32_t idx_doc, float* rcp)
 /* A leaf's posting list as the reference stores it (DataBase.h:58): document ids ascending,
  * repeated once per descriptor.  *n = full length; at most `capacity` ids are written. */
 RBW_API int rbw_db_postings(const rbw_database* db, uint32_t leaf, uint32_t* out, uint32_t capacity, uint32_t* n);
+
+/* ------------------------------------------------------------------ serving
+ * No counterpart in the reference, whose application looks a query image up and queries the
+ * database one image at a time.  A server answers query images (host descriptors) with their
+ * top-k documents (lookup + scoring) and batches them continuously: a batch is formed from the
+ * waiting requests, in arrival order, as soon as one of max_inflight_batches slots is free and
+ * only while its device-memory estimate fits what the batches in flight leave of
+ * hbm_budget_bytes; each batch runs on its own stream, so batches overlap on the GPU and
+ * requests that arrive meanwhile join the next one.  Results do not depend on the batching. */
+typedef struct rbw_server rbw_server;
+
+typedef struct {
+    uint32_t max_batch_queries;     /* requests per batch (default 256) */
+    uint32_t max_inflight_batches;  /* batches on the GPU at once (default 3) */
+    uint64_t max_batch_descriptors; /* descriptors per batch (default 2^21) */
+    uint64_t hbm_budget_bytes;      /* device memory for batches; 0 = half the free memory at creation */
+    uint32_t max_results;           /* k of every request, 1..1024 (default 100) */
+} rbw_server_options;
+
+typedef struct {
+    uint64_t submitted, completed, batches;
+    uint32_t max_inflight_seen;     /* most batches on the GPU at once */
+    double mean_batch_requests;
+    double p50_ms, p99_ms, max_ms;  /* latency from submit to result, completed requests */
+} rbw_server_stats;
+
+RBW_API void rbw_server_options_default(rbw_server_options* opts);
+/* The vocabulary and database must outlive the server; documents may still be added. */
+RBW_API int rbw_server_create(const rbw_vocabulary* voc, rbw_database* db, const rbw_server_options* opts,
+                              rbw_server** out);
+/* Copies the request's descriptors (n_desc x 128 bytes, host) and returns at once. */
+RBW_API int rbw_server_submit(rbw_server* server, const void* host_desc, uint32_t n_desc, uint64_t* request_id);
+/* Waits for a request (timeout_us < 0: no limit; RBW_ERR_TIMEOUT when it runs out, and the
+ * request can be waited for again) and collects its results: up to `capacity` documents and
+ * scores, *n_out of them in all, and its latency. */
+RBW_API int rbw_server_wait(rbw_server* server, uint64_t request_id, int64_t timeout_us, uint32_t* docs,
+                            float* scores, uint32_t capacity, uint32_t* n_out, double* latency_ms);
+RBW_API int rbw_server_get_stats(rbw_server* server, rbw_server_stats* stats);
+RBW_API int rbw_server_reset_stats(rbw_server* server);
+/* The device-memory estimate the server reserves against hbm_budget_bytes for a batch of
+ * n_requests requests holding n_desc descriptors in all (for sizing the budget). */
+RBW_API int rbw_server_batch_bytes(rbw_server* server, uint64_t n_desc, uint32_t n_requests, uint64_t* bytes);
+/* Fails requests still waiting, finishes the batches in flight. */
+RBW_API void rbw_server_destroy(rbw_server* server);
 
 /* Optional CUDA-event timing of this library's own kernel launches (no reference
  * counterpart; used by bench.py).  While enabled, each launch of a timed kernel is bracketed by

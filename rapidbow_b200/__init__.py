@@ -9,6 +9,7 @@ include/rapidbow_b200.h:
     IVocabulary::serialize       -> Vocabulary.serialize()           -> bytes
     rbow::createDataBase         -> create_database(voc)             -> DataBase
     IDataBase::addDoc / query / queryAndAddDoc -> DataBase.add_doc / query / query_and_add_doc
+    (no counterpart)             -> Server(voc, db): continuous-batching retrieval serving
 
 Errors raise RbwError (the reference throws std::runtime_error).  The compiled library must be
 present: there is no CPU fallback.
@@ -21,7 +22,7 @@ from typing import Optional
 
 import numpy as np
 
-__all__ = ["RbwError", "Vocabulary", "DataBase", "build_vocabulary", "deserialize_vocabulary", "create_database",
+__all__ = ["RbwError", "Vocabulary", "DataBase", "Server", "build_vocabulary", "deserialize_vocabulary", "create_database",
            "load_library", "LIB_PATH", "SIFT_ATTR"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -113,6 +114,15 @@ def _bind_optional(lib: C.CDLL) -> None:
         "rbw_db_segments": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
         "rbw_db_doc_rcp": (C.c_int, [vp, u32, C.POINTER(C.c_float)]),
         "rbw_db_postings": (C.c_int, [vp, u32, vp, u32, C.POINTER(u32)]),
+        "rbw_db_query_batched_host_offsets": (C.c_int, [vp, vp, vp, vp, u32, u32, vp, vp, vp, vp]),
+        "rbw_server_options_default": (None, [vp]),
+        "rbw_server_create": (C.c_int, [vp, vp, vp, pp]),
+        "rbw_server_destroy": (None, [vp]),
+        "rbw_server_submit": (C.c_int, [vp, vp, u32, C.POINTER(u64)]),
+        "rbw_server_wait": (C.c_int, [vp, u64, C.c_int64, vp, vp, u32, C.POINTER(u32), C.POINTER(C.c_double)]),
+        "rbw_server_get_stats": (C.c_int, [vp, vp]),
+        "rbw_server_reset_stats": (C.c_int, [vp]),
+        "rbw_server_batch_bytes": (C.c_int, [vp, u64, u32, C.POINTER(u64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name, None)
@@ -329,3 +339,4 @@ def deserialize_vocabulary(blob: bytes) -> Vocabulary:
 
 
 from .database import DataBase, create_database  # noqa: E402
+from .server import Server  # noqa: E402

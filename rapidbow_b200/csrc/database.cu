@@ -52,7 +52,6 @@ constexpr uint32_t kSegThreads = 256;
 constexpr uint32_t kSmemDocs = 20480;     // per-document accumulators kept in shared memory
 constexpr uint32_t kMaxK = 1024;
 constexpr double kFixScale = 72057594037927936.0; // 2^56
-constexpr size_t kGlobalAccBudget = size_t(1) << 30; // accumulators of one scoring launch
 constexpr uint32_t kDeltaMinDocs = 256;   // the delta may always hold this many documents
 constexpr uint32_t kDeltaFraction = 4;    // ... or up to main / kDeltaFraction
 
@@ -304,24 +303,24 @@ struct ScoreParams {
     const float* rcpF;
     const uint32_t* slotDoc;
     uint32_t nDocs;
+    uint32_t shardDocs;        // documents per CTA (blockIdx.y selects the shard)
     uint32_t B;
     uint32_t L;
     uint32_t k;
-    uint32_t qBase;             // first query of this launch
-    unsigned long long* gAcc;   // [launch queries][nDocs] when the accumulators do not fit shared memory
-    uint8_t* gTouched;          // [launch queries][nDocs]
-    uint32_t* outDocs;          // [nq][k]
-    float* outScores;           // [nq][k]
-    uint32_t* outCount;         // [nq]
+    unsigned long long* cand;  // [nq][shards][k] candidate keys when there are several shards
+    uint32_t* outDocs;         // [nq][k]
+    float* outScores;          // [nq][k]
+    uint32_t* outCount;        // [nq]
 };
 
 __device__ __forceinline__ float termOf(float q, float d) { return fabsf(q - d) - (q + d); }
 
-__device__ __forceinline__ void addTerm(unsigned long long* acc, uint8_t* touched, uint32_t slot, float term)
+// Adds a term to a document of this CTA's shard (local index `i` < shard size).
+__device__ __forceinline__ void addTerm(unsigned long long* acc, uint8_t* touched, uint32_t i, float term)
 {
     const long long fx = llrint(static_cast<double>(term) * kFixScale);
-    atomicAdd(&acc[slot], static_cast<unsigned long long>(fx));
-    touched[slot] = 1; // every writer stores the same value
+    atomicAdd(&acc[i], static_cast<unsigned long long>(fx));
+    touched[i] = 1; // every writer stores the same value
 }
 
 // Float bits mapped so that unsigned order is numeric order (negative scores included).
@@ -335,19 +334,83 @@ __device__ __forceinline__ float fromOrderedBits(uint32_t o)
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
 }
 
+// The `want` smallest of n distinct keys (~0 = no key), ascending, into sel[0, want): radix
+// select of the want-th smallest key, 8 bits at a time, then a bitonic sort of the winners.
+// All threads of the CTA call it; keys may live in shared or global memory.
+__device__ void selectSmallest(const unsigned long long* keys, uint32_t n, uint32_t want, unsigned long long* sel)
+{
+    __shared__ uint32_t hist[256];
+    __shared__ unsigned long long prefix;
+    __shared__ uint32_t need, nSel;
+    if (threadIdx.x == 0) {
+        prefix = 0;
+        nSel = 0;
+        need = want;
+    }
+    __syncthreads();
+    if (want > 0) {
+        for (int shift = 56; shift >= 0; shift -= 8) {
+            for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+            __syncthreads();
+            const unsigned long long hiMask = shift == 56 ? 0ull : (~0ull << (shift + 8));
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const unsigned long long key = keys[i];
+                if (key != ~0ull && (key & hiMask) == prefix) atomicAdd(&hist[(key >> shift) & 0xFFu], 1u);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t c = 0, d = 0;
+                for (; d < 255; d++) {
+                    if (c + hist[d] >= need) break;
+                    c += hist[d];
+                }
+                need -= c;
+                prefix |= static_cast<unsigned long long>(d) << shift;
+            }
+            __syncthreads();
+        }
+        // prefix is the want-th smallest key; keys are distinct, so exactly `want` are <= prefix
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long key = keys[i];
+            if (key <= prefix) {
+                const uint32_t s = atomicAdd(&nSel, 1u);
+                if (s < kMaxK) sel[s] = key;
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t m = nSel < kMaxK ? nSel : kMaxK;
+    uint32_t mPow2 = 1;
+    while (mPow2 < m) mPow2 <<= 1;
+    for (uint32_t i = m + threadIdx.x; i < mPow2; i += blockDim.x) sel[i] = ~0ull;
+    __syncthreads();
+    bitonicSortShared(sel, mPow2);
+}
+
+__device__ void writeResults(const ScoreParams& P, uint32_t q, const unsigned long long* sel, uint32_t want)
+{
+    for (uint32_t i = threadIdx.x; i < want; i += blockDim.x) {
+        P.outDocs[uint64_t(q) * P.k + i] = static_cast<uint32_t>(sel[i]);
+        P.outScores[uint64_t(q) * P.k + i] = fromOrderedBits(static_cast<uint32_t>(sel[i] >> 32));
+    }
+    if (threadIdx.x == 0) P.outCount[q] = want;
+}
+
+// One CTA per (query, shard of shardDocs documents).  The accumulators of the shard live in
+// shared memory (9 B per document); every CTA of a query walks all the query's postings and
+// keeps those of its shard.
 __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
 {
     extern __shared__ unsigned long long dyn[];
-    __shared__ uint32_t hist[256];
-    __shared__ unsigned long long prefix;
-    __shared__ uint32_t need, nSel, nTouched;
+    __shared__ uint32_t nTouched;
     __shared__ unsigned long long sel[kMaxK];
-    const uint32_t local = blockIdx.x;
-    const uint32_t q = P.qBase + local;
-    const bool inSmem = P.gAcc == nullptr;
-    unsigned long long* acc = inSmem ? dyn : P.gAcc + uint64_t(local) * P.nDocs;
-    uint8_t* touched = inSmem ? reinterpret_cast<uint8_t*>(dyn + P.nDocs) : P.gTouched + uint64_t(local) * P.nDocs;
-    for (uint32_t i = threadIdx.x; i < P.nDocs; i += blockDim.x) {
+    const uint32_t q = blockIdx.x;
+    const uint32_t shard = blockIdx.y;
+    const uint32_t docBeg = shard * P.shardDocs;
+    const uint32_t nLocal = min(P.shardDocs, P.nDocs - docBeg);
+    unsigned long long* acc = dyn;
+    uint8_t* touched = reinterpret_cast<uint8_t*>(dyn + P.shardDocs);
+    for (uint32_t i = threadIdx.x; i < nLocal; i += blockDim.x) {
         acc[i] = 0;
         touched[i] = 0;
     }
@@ -377,22 +440,24 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
 #pragma unroll
                     for (int u = 0; u < 4; u++) pr[u] = pairs[p + 32 * u];
 #pragma unroll
-                    for (int u = 0; u < 4; u++)
-                        addTerm(acc, touched, static_cast<uint32_t>(pr[u] >> 32),
-                                termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
+                    for (int u = 0; u < 4; u++) {
+                        const uint32_t i = static_cast<uint32_t>(pr[u] >> 32) - docBeg;
+                        if (i < nLocal) addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
+                    }
                 }
                 for (; p < b; p += 32) {
                     const uint64_t pr = pairs[p];
-                    addTerm(acc, touched, static_cast<uint32_t>(pr >> 32),
-                            termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
+                    const uint32_t i = static_cast<uint32_t>(pr >> 32) - docBeg;
+                    if (i < nLocal) addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
                 }
             } else {
                 // Virtual inverted file of a non-leaf word: the union of the leaf lists below
                 // it, counted per document (DataBase.cpp:150-164).  A document lives in one
                 // segment only, and the skip rule keeps the union short, so each lane scans the
-                // segment's range for the documents whose first pair it holds.
+                // segment's range for the documents of this shard whose first pair it holds.
                 for (uint32_t p = a + lane; p < b; p += 32) {
                     const uint32_t slot = static_cast<uint32_t>(pairs[p] >> 32);
+                    if (slot - docBeg >= nLocal) continue;
                     bool first = true;
                     for (uint32_t r = a; r < p && first; r++) first = static_cast<uint32_t>(pairs[r] >> 32) != slot;
                     if (!first) continue;
@@ -400,7 +465,7 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
                     for (uint32_t r = p; r < b; r++)
                         if (static_cast<uint32_t>(pairs[r] >> 32) == slot) tf += P.seg[s].tf[r];
                     const float d = float(tf) * w * P.rcpF[slot];
-                    addTerm(acc, touched, slot, termOf(qv, d));
+                    addTerm(acc, touched, slot - docBeg, termOf(qv, d));
                 }
             }
         }
@@ -410,68 +475,45 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
     // Keys: ordered score bits << 32 | document id.  Ties in score go to the lower document id;
     // untouched documents get ~0.
     uint32_t myTouched = 0;
-    for (uint32_t i = threadIdx.x; i < P.nDocs; i += blockDim.x) {
+    for (uint32_t i = threadIdx.x; i < nLocal; i += blockDim.x) {
         unsigned long long key = ~0ull;
         if (touched[i]) {
             const double sum = static_cast<double>(static_cast<long long>(acc[i])) / kFixScale;
             const float score = float(sum + 2.0f);
-            key = (static_cast<unsigned long long>(orderedBits(score)) << 32) | P.slotDoc[i];
+            key = (static_cast<unsigned long long>(orderedBits(score)) << 32) | P.slotDoc[docBeg + i];
             myTouched++;
         }
         acc[i] = key;
     }
     atomicAdd(&nTouched, myTouched);
-    if (threadIdx.x == 0) {
-        prefix = 0;
-        nSel = 0;
-    }
     __syncthreads();
     const uint32_t want = P.k < nTouched ? P.k : nTouched;
-    if (threadIdx.x == 0) need = want;
-    __syncthreads();
-    if (want > 0) {
-        // radix select of the want-th smallest key, 8 bits at a time
-        for (int shift = 56; shift >= 0; shift -= 8) {
-            for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
-            __syncthreads();
-            const unsigned long long hiMask = shift == 56 ? 0ull : (~0ull << (shift + 8));
-            for (uint32_t i = threadIdx.x; i < P.nDocs; i += blockDim.x) {
-                const unsigned long long key = acc[i];
-                if (key != ~0ull && (key & hiMask) == prefix) atomicAdd(&hist[(key >> shift) & 0xFFu], 1u);
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t c = 0, d = 0;
-                for (; d < 255; d++) {
-                    if (c + hist[d] >= need) break;
-                    c += hist[d];
-                }
-                need -= c;
-                prefix |= static_cast<unsigned long long>(d) << shift;
-            }
-            __syncthreads();
-        }
-        // prefix is the want-th smallest key; keys are distinct, so exactly `want` are <= prefix
-        for (uint32_t i = threadIdx.x; i < P.nDocs; i += blockDim.x) {
-            const unsigned long long key = acc[i];
-            if (key <= prefix) {
-                const uint32_t s = atomicAdd(&nSel, 1u);
-                if (s < kMaxK) sel[s] = key;
-            }
-        }
+    selectSmallest(acc, nLocal, want, sel);
+    if (P.cand == nullptr) {
+        writeResults(P, q, sel, want);
+    } else {
+        unsigned long long* c = P.cand + (uint64_t(q) * gridDim.y + shard) * P.k;
+        for (uint32_t i = threadIdx.x; i < P.k; i += blockDim.x) c[i] = i < want ? sel[i] : ~0ull;
     }
+}
+
+// The k best of the shards' candidates of each query (one CTA per query).
+__global__ void __launch_bounds__(kScoreThreads) mergeKernel(ScoreParams P, uint32_t shards)
+{
+    __shared__ uint32_t nValid;
+    __shared__ unsigned long long sel[kMaxK];
+    const uint32_t q = blockIdx.x;
+    const unsigned long long* c = P.cand + uint64_t(q) * shards * P.k;
+    const uint32_t n = shards * P.k;
+    if (threadIdx.x == 0) nValid = 0;
     __syncthreads();
-    const uint32_t m = nSel < kMaxK ? nSel : kMaxK;
-    uint32_t mPow2 = 1;
-    while (mPow2 < m) mPow2 <<= 1;
-    for (uint32_t i = m + threadIdx.x; i < mPow2; i += blockDim.x) sel[i] = ~0ull;
+    uint32_t mine = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) mine += c[i] != ~0ull ? 1u : 0u;
+    atomicAdd(&nValid, mine);
     __syncthreads();
-    bitonicSortShared(sel, mPow2);
-    for (uint32_t i = threadIdx.x; i < want; i += blockDim.x) {
-        P.outDocs[uint64_t(q) * P.k + i] = static_cast<uint32_t>(sel[i]);
-        P.outScores[uint64_t(q) * P.k + i] = fromOrderedBits(static_cast<uint32_t>(sel[i] >> 32));
-    }
-    if (threadIdx.x == 0) P.outCount[q] = want;
+    const uint32_t want = P.k < nValid ? P.k : nValid;
+    selectSmallest(c, n, want, sel);
+    writeResults(P, q, sel, want);
 }
 
 // Device memory from the library's stream-ordered pool, grown on a stream (keeping a prefix).
@@ -655,17 +697,15 @@ public:
         }
         const uint32_t nDocs = mIndexed;
         cudaMemPool_t pool = libraryPool();
-        const bool smemAcc = nDocs <= kSmemDocs;
-        const size_t perQueryAcc = size_t(nDocs) * 9;
-        const uint32_t chunk =
-            smemAcc ? nq : static_cast<uint32_t>(std::clamp<size_t>(kGlobalAccBudget / perQueryAcc, 1, nq));
+        const uint32_t shardDocs = std::min(std::max(nDocs, 1u), kSmemDocs);
+        const uint32_t shards = std::max(1u, (nDocs + shardDocs - 1) / shardDocs);
         const size_t entBytes = std::max<uint64_t>(totalLeaves, 1) * mL * sizeof(Entry);
-        const size_t accBytes = smemAcc ? 16 : size_t(chunk) * perQueryAcc + 16;
-        void *ent = nullptr, *cnt = nullptr, *qr = nullptr, *acc = nullptr;
+        const size_t candBytes = shards > 1 ? size_t(nq) * shards * k * 8 : 16;
+        void *ent = nullptr, *cnt = nullptr, *qr = nullptr, *cand = nullptr;
         RBW_CUDA(cudaMallocFromPoolAsync(&ent, entBytes, pool, stream));
         RBW_CUDA(cudaMallocFromPoolAsync(&cnt, size_t(nq) * 4, pool, stream));
         RBW_CUDA(cudaMallocFromPoolAsync(&qr, size_t(nq) * 4, pool, stream));
-        RBW_CUDA(cudaMallocFromPoolAsync(&acc, accBytes, pool, stream));
+        RBW_CUDA(cudaMallocFromPoolAsync(&cand, candBytes, pool, stream));
         {
             ScopedKernelTimer timer(kTimedScore, stream);
             const size_t prepSmem = size_t(nextPow2(std::max(maxN, 1u))) * 4;
@@ -686,30 +726,27 @@ public:
             P.rcpF = mRcpF.as<float>();
             P.slotDoc = mSlotDoc.as<uint32_t>();
             P.nDocs = nDocs;
+            P.shardDocs = shardDocs;
             P.B = mB;
             P.L = mL;
             P.k = k;
+            P.cand = shards > 1 ? static_cast<unsigned long long*>(cand) : nullptr;
             P.outDocs = dDocs;
             P.outScores = dScores;
             P.outCount = dCount;
-            size_t smem = 0;
-            if (smemAcc) {
-                smem = size_t(nDocs) * 9;
-            } else {
-                P.gAcc = static_cast<unsigned long long*>(acc);
-                P.gTouched = reinterpret_cast<uint8_t*>(P.gAcc + size_t(chunk) * nDocs);
-            }
+            const size_t smem = size_t(shardDocs) * 9;
             RBW_CUDA(cudaFuncSetAttribute(scoreKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-            for (uint32_t q0 = 0; q0 < nq; q0 += chunk) {
-                P.qBase = q0;
-                scoreKernel<<<std::min(chunk, nq - q0), kScoreThreads, smem, stream>>>(P);
+            scoreKernel<<<dim3(nq, shards), kScoreThreads, smem, stream>>>(P);
+            RBW_CUDA(cudaGetLastError());
+            if (shards > 1) {
+                mergeKernel<<<nq, kScoreThreads, 0, stream>>>(P, shards);
                 RBW_CUDA(cudaGetLastError());
             }
         }
         RBW_CUDA(cudaFreeAsync(ent, stream));
         RBW_CUDA(cudaFreeAsync(cnt, stream));
         RBW_CUDA(cudaFreeAsync(qr, stream));
-        RBW_CUDA(cudaFreeAsync(acc, stream));
+        RBW_CUDA(cudaFreeAsync(cand, stream));
         recordQuery(stream);
     }
 

@@ -36,13 +36,16 @@ constexpr uint32_t kBBlockBytes = kNodeBytes * 17;    // node + up to 16 childre
 constexpr uint32_t kEpiWarpsPerRole = 4;              // one warp per TMEM lane quarter
 constexpr uint32_t kTcThreads = 32 * (2 + 2 * kEpiWarpsPerRole); // TMA, MMA, 4 A warps, 4 B warps
 constexpr uint32_t kSmemHistMax = 1024;
-constexpr uint32_t kTmemCols = 512;                   // children block [0,256), level-2p blocks at 256, 272
-constexpr uint32_t kTmemA = 256;
+// Two accumulator buffers of 256 columns; tile t uses buffer t & 1.  Its level-2p MMA (16
+// columns) lands in the first columns of the buffer and is read by the A warps before the
+// children MMA of the same tile overwrites the buffer.
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kTmemBuf = 256;
 constexpr uint32_t kTileCache = 1024;
 constexpr uint32_t kGatherDepth = 4;                  // gathered tiles in flight (< kStages)
 // Branch hand-off ring between A and B warps.  The A warps write tile t + kBsSlots only after the
-// level-2p MMA of that tile, which follows the children MMA of tile t + 2, which waits for the
-// B warps to release tile t + 1 -- so 4 slots never overwrite a tile the B warps still read.
+// level-2p MMA of that tile, which waits for the B warps to release buffer (t + kBsSlots) & 1,
+// i.e. to finish tile t + 2 -- so 4 slots never overwrite a tile the B warps still read.
 constexpr uint32_t kBsSlots = 4;
 
 struct TcSmem {
@@ -52,10 +55,10 @@ struct TcSmem {
     uint64_t aEmpty[kStages];
     uint64_t bFull[2];
     uint64_t bEmpty[2];
-    uint64_t accA[2];     // level-2p accumulators j complete
-    uint64_t accAFree[2]; // A warps done with level-2p buffer j
-    uint64_t accB;        // children accumulators complete (one phase per tile)
-    uint64_t accBFree;    // B warps done with the children buffer
+    uint64_t accA[2];     // level-2p MMA into buffer j complete (one phase per use of j)
+    uint64_t aRead[2];    // A warps have read the level-2p accumulators of buffer j
+    uint64_t accB[2];     // children MMA into buffer j complete
+    uint64_t bufFree[2];  // the last reader of buffer j is done with it
     uint64_t bsReady[kBsSlots]; // A warps wrote the branches of tile t into bstar[t % kBsSlots]
     uint64_t mmaDone;
     uint32_t tmemBase;
@@ -204,10 +207,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mbarInit(&S.bFull[j], 1);
             mbarInit(&S.bEmpty[j], 1 + (two ? 2u : 1u) * kEpiWarpsPerRole); // MMA commit + epilogue warps
             mbarInit(&S.accA[j], 1);
-            mbarInit(&S.accAFree[j], kEpiWarpsPerRole);
+            mbarInit(&S.aRead[j], kEpiWarpsPerRole);
+            mbarInit(&S.accB[j], 1);
+            mbarInit(&S.bufFree[j], kEpiWarpsPerRole);
         }
-        mbarInit(&S.accB, 1);
-        mbarInit(&S.accBFree, kEpiWarpsPerRole);
         for (uint32_t j = 0; j < kBsSlots; j++) mbarInit(&S.bsReady[j], kEpiWarpsPerRole);
         mbarInit(&S.mmaDone, 1);
         S.abortFlag = 0;
@@ -342,75 +345,69 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncwarp();
     } else if (nT > 0 && warp == 1) {
         // ------------------------------------------------------------ MMA issuer (one thread)
-        // TMEM: children accumulators in columns [0, 16B) (one buffer), level-2p accumulators in
-        // two 16-column buffers at 256 + 16j.  Order a0 | a1 b0 | a2 b1 | ...: the level-2p MMA of
-        // the next tile runs ahead; the children MMA of tile t waits only for the B warps to have
-        // read tile t-1's children block.  One level: a0 a1 a2 ...
+        // Tile t accumulates in TMEM buffer j = t & 1 (columns [256 j, 256 j + 256)).  Tiles go
+        // in pairs: a(t) a(t+1) b(t) b(t+1) a(t+2) ...  a(t) (level 2p, 16 columns) needs the
+        // buffer released by the readers of tile t-2; b(t) (children, 16 B columns) overwrites
+        // the same buffer once the A warps have read a(t).  While the epilogue warps read one
+        // buffer the tensor pipe works on the other.  One level: a(t) only, in the same buffers.
+        // (Issuing out of this order, b(t) as soon as a(t) was read, measured slower.)
         if (lane == 0) {
             const uint32_t idescA = idescU8(16);
             const uint32_t idescB = idescU8(16 * p.B);
-            uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, uses0 = 0, uses1 = 0, slotOf0 = 0, slotOf1 = 0;
+            uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, uses0 = 0, uses1 = 0;
+            uint32_t slotOf[2] = {0, 0};
             bool ok = true;
-            const uint32_t nSteps = two ? 2 * nT + 1 : nT; // b(nT-1) is step 2nT
-            for (uint32_t k = 0; ok && k < nSteps; k++) {
-                uint32_t t;
-                bool isA;
-                if (!two) {
-                    t = k;
-                    isA = true;
-                } else if (k == 0) {
-                    t = 0;
-                    isA = true;
-                } else {
-                    // k = 1, 2, 3, ... -> a1 b0 a2 b1 a3 b2 ...
-                    isA = (k & 1u) != 0;
-                    t = isA ? (k + 1u) / 2u : k / 2u - 1u;
-                    if (isA && t >= nT) continue;
-                }
+            auto issueA = [&](uint32_t t) -> bool {
+                const uint32_t j = t & 1u;
                 const uint32_t s = t % kStages;
                 const TileInfo ti = tileAtSmem(S, p, t0, t);
-                if (isA) {
-                    const uint32_t j = t & 1u;
-                    if (ti.group != prevGroup) {
-                        slot ^= 1u;
-                        const uint32_t u = slot ? uses1++ : uses0++;
-                        ok = mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 20);
-                        if (!ok) break;
-                        prevGroup = ti.group;
-                    }
-                    if (j) slotOf1 = slot; else slotOf0 = slot;
-                    ok = mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21);
-                    if (ok && t >= 2) ok = mbarWait(&S.accAFree[j], ((t >> 1) - 1u) & 1u, abortFlag, p.err, 22);
-                    if (!ok) break;
-                    tcFenceAfter();
-                    const uint32_t aBase = smemAddr(S.a[s]);
-                    const uint32_t bBase = smemAddr(S.b[slot]);
-#pragma unroll
-                    for (uint32_t q4 = 0; q4 < 4; q4++) {
-                        mmaU8(tmem + kTmemA + 16u * j, smemDescSw128(aBase + 32u * q4),
-                              smemDescSw128(bBase + 32u * q4), idescA, q4 > 0 ? 1u : 0u);
-                    }
-                    mmaCommit(&S.accA[j]);
-                    if (!two) {
-                        mmaCommit(&S.aEmpty[s]);
-                        if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[slot]);
-                    }
-                } else {
-                    const uint32_t sl = (t & 1u) ? slotOf1 : slotOf0;
-                    if (t >= 1) ok = mbarWait(&S.accBFree, (t - 1u) & 1u, abortFlag, p.err, 23);
-                    if (!ok) break;
-                    tcFenceAfter();
-                    const uint32_t aBase = smemAddr(S.a[s]);
-                    const uint32_t bBase = smemAddr(S.b[sl]) + kNodeBytes;
-#pragma unroll
-                    for (uint32_t q4 = 0; q4 < 4; q4++) {
-                        mmaU8(tmem, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4), idescB,
-                              q4 > 0 ? 1u : 0u);
-                    }
-                    mmaCommit(&S.accB);
-                    mmaCommit(&S.aEmpty[s]);
-                    if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[sl]);
+                if (ti.group != prevGroup) {
+                    slot ^= 1u;
+                    const uint32_t u = slot ? uses1++ : uses0++;
+                    if (!mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 20)) return false;
+                    prevGroup = ti.group;
                 }
+                slotOf[j] = slot;
+                if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21)) return false;
+                if (t >= 2 && !mbarWait(&S.bufFree[j], ((t >> 1) - 1u) & 1u, abortFlag, p.err, 22)) return false;
+                tcFenceAfter();
+                const uint32_t aBase = smemAddr(S.a[s]);
+                const uint32_t bBase = smemAddr(S.b[slot]);
+#pragma unroll
+                for (uint32_t q4 = 0; q4 < 4; q4++) {
+                    mmaU8(tmem + kTmemBuf * j, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4),
+                          idescA, q4 > 0 ? 1u : 0u);
+                }
+                mmaCommit(&S.accA[j]);
+                if (!two) {
+                    mmaCommit(&S.aEmpty[s]);
+                    if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[slot]);
+                }
+                return true;
+            };
+            auto issueB = [&](uint32_t t) -> bool {
+                const uint32_t j = t & 1u;
+                const uint32_t s = t % kStages;
+                const uint32_t sl = slotOf[j];
+                if (!mbarWait(&S.aRead[j], (t >> 1) & 1u, abortFlag, p.err, 23)) return false;
+                tcFenceAfter();
+                const uint32_t aBase = smemAddr(S.a[s]);
+                const uint32_t bBase = smemAddr(S.b[sl]) + kNodeBytes;
+#pragma unroll
+                for (uint32_t q4 = 0; q4 < 4; q4++) {
+                    mmaU8(tmem + kTmemBuf * j, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4),
+                          idescB, q4 > 0 ? 1u : 0u);
+                }
+                mmaCommit(&S.accB[j]);
+                mmaCommit(&S.aEmpty[s]);
+                if (lastOfGroupSmem(S, p, t0, nT, t, tileAtSmem(S, p, t0, t).group)) mmaCommit(&S.bEmpty[sl]);
+                return true;
+            };
+            for (uint32_t t = 0; ok && t < nT; t += 2) {
+                ok = issueA(t);
+                if (ok && t + 1 < nT) ok = issueA(t + 1);
+                if (ok && two) ok = issueB(t);
+                if (ok && two && t + 1 < nT) ok = issueB(t + 1);
             }
             mmaCommit(&S.mmaDone);
             mbarWait(&S.mmaDone, 0, abortFlag, p.err, 24);
@@ -420,7 +417,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // ------------------------------------------------------------ A warps: level-2p argmin
         // One warp per TMEM lane quarter; each thread owns one tile row.  With two levels the
         // branch is handed to the B warps through shared memory (written before the arrival
-        // the B warps wait on).
+        // the B warps wait on), and the buffer goes on to the children MMA; with one level the
+        // A warps are its last readers.
         const uint32_t q = warp & 3u;
         const uint32_t row = q * 32u + lane;
         const uint32_t tRow = tmem + ((q * 32u) << 16);
@@ -436,15 +434,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (!mbarWait(&S.accA[j], (t >> 1) & 1u, abortFlag, p.err, 30)) break;
             tcFenceAfter();
             uint32_t r[16];
-            tmemLoad16(tRow + kTmemA + 16u * j, r);
+            tmemLoad16(tRow + kTmemBuf * j, r);
             tmemWaitTie(r);
             const uint32_t b = argminScores(r, &S.cn[slot][0][0]);
             if (two) S.bstar[t % kBsSlots][row] = static_cast<uint8_t>(b);
             tcFenceBefore();
             __syncwarp();
             if (lane == 0) {
-                mbarArrive(&S.accAFree[j]);
-                if (two) mbarArrive(&S.bsReady[t % kBsSlots]);
+                if (two) {
+                    mbarArrive(&S.aRead[j]);
+                    mbarArrive(&S.bsReady[t % kBsSlots]);
+                } else {
+                    mbarArrive(&S.bufFree[j]);
+                }
             }
             if (!two && row < ti.count) emitRow(S, p, smemHist, orig, ti.group * p.B + b);
             if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) {
@@ -468,7 +470,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 prevGroup = ti.group;
             }
             const uint32_t orig = row < ti.count ? (gather ? __ldg(p.perm + ti.start + row) : ti.start + row) : 0u;
-            if (!mbarWait(&S.accB, t & 1u, abortFlag, p.err, 31)) break;
+            if (!mbarWait(&S.accB[j], (t >> 1) & 1u, abortFlag, p.err, 31)) break;
             // acquire the A warps' branch writes for this tile
             if (!mbarWait(&S.bsReady[t % kBsSlots], (t / kBsSlots) & 1u, abortFlag, p.err, 32)) break;
             tcFenceAfter();
@@ -477,21 +479,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
             for (int i = 0; i < 16; i++) sel[i] = 0;
             {
+                const uint32_t base = tRow + kTmemBuf * j;
                 uint32_t r[128];
-                tmemLoad128(tRow, r);
+                tmemLoad128(base, r);
                 tmemWaitTie128(r);
                 if (p.B > 8) {
 #pragma unroll
                     for (uint32_t k = 0; k < 8; k++)
 #pragma unroll
                         for (int i = 0; i < 16; i++) sel[i] = bs == k ? r[16 * k + i] : sel[i];
-                    tmemLoad128(tRow + 128u, r);
+                    tmemLoad128(base + 128u, r);
                     tmemWaitTie128(r);
                 }
-                // the accumulators are in registers: let the next tile's children MMA run
+                // the accumulators are in registers: the buffer can take tile t + 2
                 tcFenceBefore();
                 __syncwarp();
-                if (lane == 0) mbarArrive(&S.accBFree);
+                if (lane == 0) mbarArrive(&S.bufFree[j]);
                 const uint32_t k0 = p.B > 8 ? 8u : 0u;
 #pragma unroll
                 for (uint32_t k = 0; k < 8; k++)

@@ -1,9 +1,9 @@
 // Lookup that allocates nothing.
 //
-// Some callers cannot allocate device memory when they look descriptors up: code running
-// while a CUDA graph is being captured, real-time or serving loops that must not hit the
-// driver allocator (cudaMalloc can synchronise the device and its latency is unbounded), and
-// hosts that hand this library a fixed memory budget up front.  For them,
+// Some callers cannot allocate device memory when they look descriptors up: real-time or
+// serving loops that must not hit the driver allocator (cudaMalloc can synchronise the device
+// and its latency is unbounded), plug-ins running inside a host application that owns all GPU
+// memory, and hosts that hand this library a fixed memory budget up front.  For them,
 // rbw_voc_lookup_noalloc runs the same tensor-core lookup as rbw_voc_lookup, but its working
 // memory (the regroup permutation, histograms and tile lists between passes) lives in one
 // file-scope device array of kNoAllocScratchBytes, reserved on every GPU that loads this

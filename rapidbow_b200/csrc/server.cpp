@@ -1,0 +1,460 @@
+// Retrieval serving loop: continuous batching of query images over a device-resident DataBase.
+//
+// A request is one query image's descriptors (host memory).  Requests are answered with the
+// image's top-k database documents, computed as the reference's application does it: the
+// descriptors are looked up to leaf words (IVocabulary::lookUp, Vocabulary.cpp:162-173) and the
+// words scored against the inverted file (DataBase::query, DataBase.cpp:71-190).
+//
+// Batching: a dispatcher thread forms a batch from the pending requests, in arrival order, as
+// soon as a batch slot is free, up to the slot's request and descriptor limits and only while
+// the batch's device memory estimate fits the memory budget left by the batches in flight
+// (admission by free HBM).  A batch copies its descriptors in, looks them up and scores all its
+// requests in one scoring launch, on its own stream, so up to max_inflight batches overlap on
+// the GPU; requests that arrive meanwhile join the next batch.  A completion thread waits for
+// each batch in order, hands the results to the requests and frees the slot.
+//
+// Results do not depend on how requests were batched: the lookup is exact and every query is
+// scored independently with an order-independent sum.
+#include "capi_internal.h"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace rbw {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    std::vector<uint8_t> desc;   // n x 128
+    uint32_t n = 0;
+    Clock::time_point submitted, finished;
+    bool done = false;
+    int status = 0;
+    std::string error;
+    std::vector<uint32_t> docs;
+    std::vector<float> scores;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    uint8_t* hDesc = nullptr;     // pinned [maxDesc][128]
+    uint64_t* hOff = nullptr;     // pinned [maxQueries + 1]
+    uint32_t* hDocs = nullptr;    // pinned [maxQueries][k]
+    float* hScores = nullptr;     // pinned [maxQueries][k]
+    uint32_t* hCount = nullptr;   // pinned [maxQueries]
+    std::vector<std::shared_ptr<Request>> reqs;
+    size_t reserved = 0;
+    bool busy = false;
+    int status = 0;
+    std::string error;
+};
+
+class Server
+{
+public:
+    Server(const rbw_vocabulary* voc, rbw_database* db, const rbw_server_options& o) : mVoc{voc}, mDb{db}, mOpt{o}
+    {
+        if (mOpt.max_batch_queries == 0 || mOpt.max_batch_descriptors == 0 || mOpt.max_inflight_batches == 0)
+            throw Error(kInvalidArg, "server limits must be positive");
+        if (mOpt.max_results == 0 || mOpt.max_results > 1024) throw Error(kUnsupported, "max_results must be 1..1024");
+        RBW_CUDA(cudaGetDevice(&mDevice));
+        const Vocabulary& v = vocabularyOf(voc);
+        mLevels = v.levels();
+        if (mOpt.hbm_budget_bytes == 0) {
+            size_t freeB = 0, totalB = 0;
+            RBW_CUDA(cudaMemGetInfo(&freeB, &totalB));
+            mOpt.hbm_budget_bytes = freeB / 2;
+        }
+        uint32_t nDocs = 0;
+        if (rbw_db_info(db, &nDocs, nullptr) != RBW_OK) throw Error(kInvalidArg, rbw_last_error());
+        mSlots.resize(mOpt.max_inflight_batches);
+        const size_t q = mOpt.max_batch_queries, k = mOpt.max_results;
+        for (Slot& s : mSlots) {
+            RBW_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+            RBW_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+            RBW_CUDA(cudaMallocHost(&s.hDesc, mOpt.max_batch_descriptors * 128));
+            RBW_CUDA(cudaMallocHost(&s.hOff, (q + 1) * 8));
+            RBW_CUDA(cudaMallocHost(&s.hDocs, q * k * 4));
+            RBW_CUDA(cudaMallocHost(&s.hScores, q * k * 4));
+            RBW_CUDA(cudaMallocHost(&s.hCount, q * 4));
+        }
+        mDispatcher = std::thread([this] { dispatchLoop(); });
+        mCompleter = std::thread([this] { completeLoop(); });
+    }
+
+    ~Server()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mMu);
+            mStop = true;
+        }
+        mCv.notify_all();
+        mDispatcher.join();
+        mCompleter.join();
+        for (Slot& s : mSlots) {
+            cudaStreamSynchronize(s.stream);
+            cudaFreeHost(s.hDesc);
+            cudaFreeHost(s.hOff);
+            cudaFreeHost(s.hDocs);
+            cudaFreeHost(s.hScores);
+            cudaFreeHost(s.hCount);
+            cudaEventDestroy(s.done);
+            cudaStreamDestroy(s.stream);
+        }
+    }
+
+    uint64_t submit(const uint8_t* desc, uint32_t n)
+    {
+        if (n && desc == nullptr) throw Error(kInvalidArg, "null descriptors");
+        if (n > mOpt.max_batch_descriptors) throw Error(kInvalidArg, "request larger than a batch");
+        if (n > 32768) throw Error(kUnsupported, "a query may hold at most 32768 descriptors");
+        if (estimate(n, 1) > mOpt.hbm_budget_bytes) throw Error(kOutOfMemory, "request larger than the memory budget");
+        auto r = std::make_shared<Request>();
+        r->desc.assign(desc, desc + size_t(n) * 128);
+        r->n = n;
+        std::lock_guard<std::mutex> lk(mMu);
+        if (mStop) throw Error(kInvalidArg, "server stopped");
+        r->id = ++mNextId;
+        r->submitted = Clock::now();
+        mPending.push_back(r);
+        mAll.emplace(r->id, r);
+        mSubmitted++;
+        mCv.notify_all();
+        return r->id;
+    }
+
+    // Waits for a request (timeout_us < 0: no limit).  Returns false on timeout.
+    bool wait(uint64_t id, int64_t timeoutUs, uint32_t* docs, float* scores, uint32_t capacity, uint32_t* nOut,
+              double* latencyMs)
+    {
+        std::unique_lock<std::mutex> lk(mMu);
+        auto it = mAll.find(id);
+        if (it == mAll.end()) throw Error(kInvalidArg, "unknown request id (already collected?)");
+        std::shared_ptr<Request> r = it->second;
+        auto ready = [&] { return r->done; };
+        if (timeoutUs < 0) {
+            mDoneCv.wait(lk, ready);
+        } else if (!mDoneCv.wait_for(lk, std::chrono::microseconds(timeoutUs), ready)) {
+            return false;
+        }
+        mAll.erase(it);
+        if (r->status != RBW_OK) throw Error(static_cast<Status>(r->status), r->error);
+        const uint32_t n = static_cast<uint32_t>(r->docs.size());
+        if (nOut) *nOut = n;
+        const uint32_t m = std::min(n, capacity);
+        if (docs) std::memcpy(docs, r->docs.data(), size_t(m) * 4);
+        if (scores) std::memcpy(scores, r->scores.data(), size_t(m) * 4);
+        if (latencyMs) *latencyMs = std::chrono::duration<double, std::milli>(r->finished - r->submitted).count();
+        return true;
+    }
+
+    void stats(rbw_server_stats* st)
+    {
+        std::lock_guard<std::mutex> lk(mMu);
+        std::memset(st, 0, sizeof(*st));
+        st->submitted = mSubmitted;
+        st->completed = mLatencies.size();
+        st->batches = mBatches;
+        st->max_inflight_seen = mMaxInflight;
+        st->mean_batch_requests = mBatches ? double(mBatchedRequests) / double(mBatches) : 0.0;
+        if (!mLatencies.empty()) {
+            std::vector<double> l = mLatencies;
+            auto pct = [&](double p) {
+                const size_t i = std::min(l.size() - 1, static_cast<size_t>(p * double(l.size() - 1) + 0.5));
+                std::nth_element(l.begin(), l.begin() + i, l.end());
+                return l[i];
+            };
+            st->p50_ms = pct(0.50);
+            st->p99_ms = pct(0.99);
+            st->max_ms = *std::max_element(l.begin(), l.end());
+        }
+    }
+
+    size_t batchBytes(uint64_t desc, uint64_t queries) const { return estimate(desc, queries); }
+
+    void resetStats()
+    {
+        std::lock_guard<std::mutex> lk(mMu);
+        mLatencies.clear();
+        mBatches = mBatchedRequests = 0;
+        mMaxInflight = 0;
+        mSubmitted = 0;
+    }
+
+private:
+    // Device bytes a batch of `desc` descriptors in `queries` requests needs: descriptors and
+    // leaves, lookup working memory, scoring entries, results and the per-shard candidates of
+    // databases larger than one shard of 20,480 documents, plus 1 MiB of slack.
+    size_t estimate(uint64_t desc, uint64_t queries) const
+    {
+        uint64_t scratch = 0;
+        rbw_voc_lookup_scratch_bytes(mVoc, desc, &scratch);
+        uint32_t nDocs = 0;
+        rbw_db_info(mDb, &nDocs, nullptr);
+        const uint64_t shards = (uint64_t(nDocs) + 20479) / 20480;
+        const uint64_t cand = shards > 1 ? queries * shards * mOpt.max_results * 8ull : 0;
+        return size_t(desc * (128 + 4 + 16ull * mLevels) + scratch + queries * (mOpt.max_results * 8ull + 32) + cand +
+                      (1u << 20));
+    }
+
+    void dispatchLoop()
+    {
+        cudaSetDevice(mDevice);
+        for (;;) {
+            std::unique_lock<std::mutex> lk(mMu);
+            Slot* slot = nullptr;
+            mCv.wait(lk, [&] {
+                if (mStop) return true;
+                if (mPending.empty()) return false;
+                slot = freeSlot();
+                return slot != nullptr && estimate(mPending.front()->n, 1) + mReserved <= mOpt.hbm_budget_bytes;
+            });
+            if (mStop) {
+                for (auto& r : mPending) finishLocked(*r, RBW_ERR_INVALID_ARG, "server stopped");
+                mPending.clear();
+                mDoneCv.notify_all();
+                mCv.notify_all();
+                return;
+            }
+            // form the batch: arrival order, within the slot limits and the memory budget
+            uint64_t desc = 0;
+            slot->reqs.clear();
+            while (!mPending.empty() && slot->reqs.size() < mOpt.max_batch_queries) {
+                const auto& r = mPending.front();
+                if (desc + r->n > mOpt.max_batch_descriptors) break;
+                if (estimate(desc + r->n, slot->reqs.size() + 1) + mReserved > mOpt.hbm_budget_bytes) break;
+                desc += r->n;
+                slot->reqs.push_back(r);
+                mPending.pop_front();
+            }
+            slot->reserved = estimate(desc, slot->reqs.size());
+            mReserved += slot->reserved;
+            slot->busy = true;
+            mBatches++;
+            mBatchedRequests += slot->reqs.size();
+            const uint32_t inflight = static_cast<uint32_t>(
+                std::count_if(mSlots.begin(), mSlots.end(), [](const Slot& s) { return s.busy; }));
+            mMaxInflight = std::max(mMaxInflight, inflight);
+            lk.unlock();
+            launch(*slot, desc);
+            lk.lock();
+            mInflight.push_back(slot);
+            mCv.notify_all();
+        }
+    }
+
+    Slot* freeSlot()
+    {
+        for (Slot& s : mSlots)
+            if (!s.busy) return &s;
+        return nullptr;
+    }
+
+    // Copies the batch in, looks it up and scores it on the slot's stream (asynchronous).
+    void launch(Slot& s, uint64_t desc)
+    {
+        s.status = RBW_OK;
+        s.error.clear();
+        const uint32_t nq = static_cast<uint32_t>(s.reqs.size());
+        const uint32_t k = mOpt.max_results;
+        uint64_t off = 0;
+        for (uint32_t i = 0; i < nq; i++) {
+            s.hOff[i] = off;
+            if (s.reqs[i]->n) std::memcpy(s.hDesc + off * 128, s.reqs[i]->desc.data(), size_t(s.reqs[i]->n) * 128);
+            off += s.reqs[i]->n;
+        }
+        s.hOff[nq] = off;
+        void* dev = nullptr;
+        const size_t descBytes = std::max<uint64_t>(desc, 1) * 128;
+        const size_t leafBytes = (std::max<uint64_t>(desc, 1) * 4 + 7) & ~size_t(7);
+        const size_t total = descBytes + leafBytes + (size_t(nq) + 1) * 8 + size_t(nq) * k * 8 + size_t(nq) * 4 + 256;
+        try {
+            RBW_CUDA(cudaMallocFromPoolAsync(&dev, total, libraryPool(), s.stream));
+            uint8_t* dDesc = static_cast<uint8_t*>(dev);
+            uint32_t* dLeaf = reinterpret_cast<uint32_t*>(dDesc + descBytes);
+            uint64_t* dOff = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(dLeaf) + leafBytes);
+            uint32_t* dDocs = reinterpret_cast<uint32_t*>(dOff + nq + 1);
+            float* dScores = reinterpret_cast<float*>(dDocs + size_t(nq) * k);
+            uint32_t* dCount = reinterpret_cast<uint32_t*>(dScores + size_t(nq) * k);
+            if (desc) RBW_CUDA(cudaMemcpyAsync(dDesc, s.hDesc, desc * 128, cudaMemcpyHostToDevice, s.stream));
+            RBW_CUDA(cudaMemcpyAsync(dOff, s.hOff, (size_t(nq) + 1) * 8, cudaMemcpyHostToDevice, s.stream));
+            uint32_t kernels = 0;
+            int rc = desc ? rbw_voc_lookup_ex(mVoc, dDesc, desc, dLeaf, RBW_LOOKUP_AUTO, s.stream, &kernels) : RBW_OK;
+            if (rc != RBW_OK) throw Error(static_cast<Status>(rc), rbw_last_error());
+            rc = rbw_db_query_batched_host_offsets(mDb, dLeaf, dOff, s.hOff, nq, k, dDocs, dScores, dCount, s.stream);
+            if (rc != RBW_OK) throw Error(static_cast<Status>(rc), rbw_last_error());
+            RBW_CUDA(cudaMemcpyAsync(s.hDocs, dDocs, size_t(nq) * k * 4, cudaMemcpyDeviceToHost, s.stream));
+            RBW_CUDA(cudaMemcpyAsync(s.hScores, dScores, size_t(nq) * k * 4, cudaMemcpyDeviceToHost, s.stream));
+            RBW_CUDA(cudaMemcpyAsync(s.hCount, dCount, size_t(nq) * 4, cudaMemcpyDeviceToHost, s.stream));
+            RBW_CUDA(cudaFreeAsync(dev, s.stream));
+            dev = nullptr;
+        } catch (const Error& e) {
+            s.status = e.status;
+            s.error = e.what();
+        } catch (const std::exception& e) {
+            s.status = RBW_ERR_INTERNAL;
+            s.error = e.what();
+        }
+        if (dev) cudaFreeAsync(dev, s.stream);
+        cudaEventRecord(s.done, s.stream);
+    }
+
+    void completeLoop()
+    {
+        cudaSetDevice(mDevice);
+        for (;;) {
+            Slot* s = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mMu);
+                mCv.wait(lk, [&] { return !mInflight.empty() || (mStop && mPending.empty()); });
+                if (mInflight.empty()) return;
+                s = mInflight.front();
+            }
+            const cudaError_t e = cudaEventSynchronize(s->done);
+            std::lock_guard<std::mutex> lk(mMu);
+            mInflight.pop_front();
+            const uint32_t k = mOpt.max_results;
+            for (size_t i = 0; i < s->reqs.size(); i++) {
+                Request& r = *s->reqs[i];
+                if (s->status != RBW_OK || e != cudaSuccess) {
+                    finishLocked(r, s->status != RBW_OK ? s->status : RBW_ERR_CUDA,
+                                 s->status != RBW_OK ? s->error : cudaGetErrorString(e));
+                    continue;
+                }
+                const uint32_t n = std::min(s->hCount[i], k);
+                r.docs.assign(s->hDocs + i * k, s->hDocs + i * k + n);
+                r.scores.assign(s->hScores + i * k, s->hScores + i * k + n);
+                finishLocked(r, RBW_OK, "");
+            }
+            s->reqs.clear();
+            mReserved -= s->reserved;
+            s->reserved = 0;
+            s->busy = false;
+            mDoneCv.notify_all();
+            mCv.notify_all();
+        }
+    }
+
+    void finishLocked(Request& r, int status, const std::string& err)
+    {
+        r.status = status;
+        r.error = err;
+        r.finished = Clock::now();
+        r.done = true;
+        r.desc.clear();
+        r.desc.shrink_to_fit();
+        if (status == RBW_OK)
+            mLatencies.push_back(std::chrono::duration<double, std::milli>(r.finished - r.submitted).count());
+    }
+
+    const rbw_vocabulary* mVoc;
+    rbw_database* mDb;
+    rbw_server_options mOpt;
+    int mDevice = 0;
+    uint32_t mLevels = 0;
+    std::vector<Slot> mSlots;
+    std::deque<std::shared_ptr<Request>> mPending;
+    std::deque<Slot*> mInflight;
+    std::unordered_map<uint64_t, std::shared_ptr<Request>> mAll;
+    std::vector<double> mLatencies;
+    uint64_t mNextId = 0, mSubmitted = 0, mBatches = 0, mBatchedRequests = 0;
+    uint32_t mMaxInflight = 0;
+    size_t mReserved = 0;
+    bool mStop = false;
+    std::mutex mMu;
+    std::condition_variable mCv, mDoneCv;
+    std::thread mDispatcher, mCompleter;
+};
+
+} // namespace
+} // namespace rbw
+
+struct rbw_server {
+    std::unique_ptr<rbw::Server> s;
+};
+
+namespace {
+rbw::Server& serverOf(rbw_server* h)
+{
+    if (h == nullptr || !h->s) throw rbw::Error(rbw::kInvalidArg, "null server handle");
+    return *h->s;
+}
+} // namespace
+
+extern "C" {
+
+void rbw_server_options_default(rbw_server_options* o)
+{
+    if (o == nullptr) return;
+    o->max_batch_queries = 256;
+    o->max_batch_descriptors = 1u << 21;
+    o->max_inflight_batches = 3;
+    o->max_results = 100;
+    o->hbm_budget_bytes = 0;
+}
+
+int rbw_server_create(const rbw_vocabulary* voc, rbw_database* db, const rbw_server_options* opts, rbw_server** out)
+{
+    return rbw::runGuarded([&] {
+        if (out == nullptr || db == nullptr) throw rbw::Error(rbw::kInvalidArg, "null argument");
+        *out = nullptr;
+        rbw_server_options o;
+        rbw_server_options_default(&o);
+        if (opts) o = *opts;
+        *out = new rbw_server{std::make_unique<rbw::Server>(voc, db, o)};
+    });
+}
+
+void rbw_server_destroy(rbw_server* s) { delete s; }
+
+int rbw_server_submit(rbw_server* s, const void* host_desc, uint32_t n_desc, uint64_t* request_id)
+{
+    return rbw::runGuarded([&] {
+        if (request_id == nullptr) throw rbw::Error(rbw::kInvalidArg, "null request id");
+        *request_id = serverOf(s).submit(static_cast<const uint8_t*>(host_desc), n_desc);
+    });
+}
+
+int rbw_server_wait(rbw_server* s, uint64_t request_id, int64_t timeout_us, uint32_t* docs, float* scores,
+                    uint32_t capacity, uint32_t* n_out, double* latency_ms)
+{
+    return rbw::runGuarded([&] {
+        if (!serverOf(s).wait(request_id, timeout_us, docs, scores, capacity, n_out, latency_ms))
+            throw rbw::Error(rbw::kTimeout, "request not finished within the timeout");
+    });
+}
+
+int rbw_server_get_stats(rbw_server* s, rbw_server_stats* stats)
+{
+    return rbw::runGuarded([&] {
+        if (stats == nullptr) throw rbw::Error(rbw::kInvalidArg, "null stats");
+        serverOf(s).stats(stats);
+    });
+}
+
+int rbw_server_batch_bytes(rbw_server* s, uint64_t n_desc, uint32_t n_requests, uint64_t* bytes)
+{
+    return rbw::runGuarded([&] {
+        if (bytes == nullptr) throw rbw::Error(rbw::kInvalidArg, "null output");
+        *bytes = serverOf(s).batchBytes(n_desc, n_requests);
+    });
+}
+
+int rbw_server_reset_stats(rbw_server* s)
+{
+    return rbw::runGuarded([&] { serverOf(s).resetStats(); });
+}
+
+} // extern "C"

@@ -1,5 +1,6 @@
 """rbw_voc_lookup_noalloc: the lookup for callers that cannot allocate device memory during the
-call (graph capture, latency-bound serving loops, fixed memory budgets).  Its working memory is a
+call (latency-bound serving loops, plug-ins inside an application that owns the GPU memory,
+fixed memory budgets).  Its working memory is a
 fixed array inside the library, shared by all calls on a GPU and kept between calls, so two
 calls in a row must each give the same leaf IDs as the allocating entry point.  This file is
 collected last so that a run stopping at the first failure has already run every other test."""
