@@ -337,7 +337,7 @@ __device__ __forceinline__ float fromOrderedBits(uint32_t o)
 // The `want` smallest of n distinct keys (~0 = no key), ascending, into sel[0, want): radix
 // select of the want-th smallest key, 8 bits at a time, then a bitonic sort of the winners.
 // All threads of the CTA call it; keys may live in shared or global memory.
-__device__ void selectSmallest(const unsigned long long* keys, uint32_t n, uint32_t want, unsigned long long* sel)
+__device__ __forceinline__ void selectSmallest(const unsigned long long* keys, uint32_t n, uint32_t want, unsigned long long* sel)
 {
     __shared__ uint32_t hist[256];
     __shared__ unsigned long long prefix;
@@ -387,7 +387,7 @@ __device__ void selectSmallest(const unsigned long long* keys, uint32_t n, uint3
     bitonicSortShared(sel, mPow2);
 }
 
-__device__ void writeResults(const ScoreParams& P, uint32_t q, const unsigned long long* sel, uint32_t want)
+__device__ __forceinline__ void writeResults(const ScoreParams& P, uint32_t q, const unsigned long long* sel, uint32_t want)
 {
     for (uint32_t i = threadIdx.x; i < want; i += blockDim.x) {
         P.outDocs[uint64_t(q) * P.k + i] = static_cast<uint32_t>(sel[i]);
@@ -398,17 +398,22 @@ __device__ void writeResults(const ScoreParams& P, uint32_t q, const unsigned lo
 
 // One CTA per (query, shard of shardDocs documents).  The accumulators of the shard live in
 // shared memory (9 B per document); every CTA of a query walks all the query's postings and
-// keeps those of its shard.
-__global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
+// keeps those of its shard.  kSharded = false: one shard holds every document and no posting
+// needs the shard test.
+template <bool kSharded>
+__global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
 {
     extern __shared__ unsigned long long dyn[];
     __shared__ uint32_t nTouched;
     __shared__ unsigned long long sel[kMaxK];
     const uint32_t q = blockIdx.x;
     const uint32_t shard = blockIdx.y;
-    const uint32_t docBeg = shard * P.shardDocs;
-    const uint32_t nLocal = min(P.shardDocs, P.nDocs - docBeg);
-    unsigned long long* acc = dyn;
+    const uint32_t docBeg = kSharded ? shard * P.shardDocs : 0u;
+    const uint32_t nLocal = kSharded ? min(P.shardDocs, P.nDocs - docBeg) : P.nDocs;
+    // Accumulators through a generic pointer: the 64-bit atomics on it measured faster than
+    // the shared-window form the compiler picks for a known shared-memory address.
+    unsigned long long* acc;
+    asm("mov.b64 %0, %1;" : "=l"(acc) : "l"(reinterpret_cast<unsigned long long*>(dyn)));
     uint8_t* touched = reinterpret_cast<uint8_t*>(dyn + P.shardDocs);
     for (uint32_t i = threadIdx.x; i < nLocal; i += blockDim.x) {
         acc[i] = 0;
@@ -442,13 +447,15 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
                         const uint32_t i = static_cast<uint32_t>(pr[u] >> 32) - docBeg;
-                        if (i < nLocal) addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
+                        if (!kSharded || i < nLocal)
+                            addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
                     }
                 }
                 for (; p < b; p += 32) {
                     const uint64_t pr = pairs[p];
                     const uint32_t i = static_cast<uint32_t>(pr >> 32) - docBeg;
-                    if (i < nLocal) addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
+                    if (!kSharded || i < nLocal)
+                        addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
                 }
             } else {
                 // Virtual inverted file of a non-leaf word: the union of the leaf lists below
@@ -457,7 +464,7 @@ __global__ void __launch_bounds__(kScoreThreads) scoreKernel(ScoreParams P)
                 // segment's range for the documents of this shard whose first pair it holds.
                 for (uint32_t p = a + lane; p < b; p += 32) {
                     const uint32_t slot = static_cast<uint32_t>(pairs[p] >> 32);
-                    if (slot - docBeg >= nLocal) continue;
+                    if (kSharded && slot - docBeg >= nLocal) continue;
                     bool first = true;
                     for (uint32_t r = a; r < p && first; r++) first = static_cast<uint32_t>(pairs[r] >> 32) != slot;
                     if (!first) continue;
@@ -735,8 +742,13 @@ public:
             P.outScores = dScores;
             P.outCount = dCount;
             const size_t smem = size_t(shardDocs) * 9;
-            RBW_CUDA(cudaFuncSetAttribute(scoreKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-            scoreKernel<<<dim3(nq, shards), kScoreThreads, smem, stream>>>(P);
+            if (shards > 1) {
+                RBW_CUDA(cudaFuncSetAttribute(scoreKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+                scoreKernel<true><<<dim3(nq, shards), kScoreThreads, smem, stream>>>(P);
+            } else {
+                RBW_CUDA(cudaFuncSetAttribute(scoreKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+                scoreKernel<false><<<nq, kScoreThreads, smem, stream>>>(P);
+            }
             RBW_CUDA(cudaGetLastError());
             if (shards > 1) {
                 mergeKernel<<<nq, kScoreThreads, 0, stream>>>(P, shards);
