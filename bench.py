@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-scoring", action="store_true", help="skip the inverted-file scoring workload")
     p.add_argument("--db-docs", type=int, default=20000, help="images in the scoring database")
+    p.add_argument("--no-build", action="store_true", help="skip the vocabulary-build workloads")
     p.add_argument("--serving", action="store_true",
                    help="also run the serving workload (1M-word tree, 100,000 images, Poisson arrivals)")
     p.add_argument("--serving-docs", type=int, default=100_000)
@@ -327,6 +328,8 @@ def run_ours(args, world, rank, local):
         torch.cuda.empty_cache()
     if not args.no_scoring:
         line["scoring"] = scoring_bench(args, voc, dev, world, rank)
+    if not args.no_build:
+        line["build"] = build_bench(args, dev, rank)
     if args.serving:
         line["serving"] = serving_bench(args, dev, rank)
     if rank == 0:
@@ -453,6 +456,72 @@ def scoring_bench(args, voc, dev, world, rank):
             voc, ids, doc_leaves, offs, queries, k, docs.cpu().numpy().view(np.uint32), counts.cpu().numpy(),
             args.cpu_seconds)
     return res
+
+
+def build_bench(args, dev, rank):
+    """Hierarchical k-means builds: config 0 (200,000 descriptors, B=16, L=3) with a CPU
+    baseline and an exactness check against the oracle, and config 2 (10M descriptors from a
+    4,096-component Zipf(1.1) mixture, B=10, L=6).  Both: seeded k-means++ init, 10 Lloyd
+    iterations.  The build API is synchronous; times are host wall clock around it."""
+    import numpy as np
+    import torch
+
+    import rapidbow_b200 as rbw
+    from oracle.pyoracle import INIT_KMEANSPP, Oracle
+    from rapidbow_b200.synth import sift_like
+
+    def timed_build(desc, B, L, reps, **kw):
+        rbw.build_vocabulary(desc, B, nb_doc=1000, nb_levels=L, init="kmeans++", seed=7, max_iterations=10, **kw)
+        times = []
+        for _ in range(reps):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            voc = rbw.build_vocabulary(desc, B, nb_doc=1000, nb_levels=L, init="kmeans++", seed=7,
+                                       max_iterations=10, **kw)
+            torch.cuda.synchronize(dev)
+            times.append(time.perf_counter() - t0)
+        return voc, statistics.median(times)
+
+    out = {}
+    c0 = sift_like(200_000, seed=11, device=dev)
+    rbw.timing_reset()
+    rbw.timing_enable(True)
+    voc0, s0 = timed_build(c0, 16, 3, 5)
+    rbw.timing_enable(False)
+    assign_ms, _ = rbw.timing_read("kmeans_assign")
+    update_ms, _ = rbw.timing_read("kmeans_update")
+    out["config0"] = {
+        "workload": "build: 200,000 SIFT-like descriptors, B=16, L=3 (4,096 words), k-means++ init, 10 Lloyd iterations",
+        "value": s0, "unit": "s", "higher_is_better": False,
+        # 1 warm-up + 5 timed builds recorded; nodes that converge early are skipped by the kernel
+        "assign_kernel_ms_per_build": assign_ms / 6, "update_kernel_ms_per_build": update_ms / 6,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        # exactness: the GPU build with IEEE center rounding equals the oracle's build
+        host = c0.cpu().numpy()
+        voc_ieee = rbw.build_vocabulary(c0, 16, nb_doc=1000, nb_levels=3, init="kmeans++", seed=7, max_iterations=10,
+                                        ieee_division=True)
+        t0 = time.perf_counter()
+        ref = Oracle().build_vocabulary(host, 1000, 16, 3, max_iter=10, init=INIT_KMEANSPP, seed=7)
+        cpu_s = time.perf_counter() - t0
+        centers, masks, weights = voc_ieee.tree()
+        out["config0"]["matches_oracle"] = bool(np.array_equal(centers, ref["centers"]) and
+                                                np.array_equal(masks, ref["masks"]))
+        out["config0"]["cpu_baseline"] = {"value": cpu_s, "unit": "s", "cores": 1, "kind": "port",
+                                          "sample": "the same build (oracle restatement, one thread)"}
+    del c0
+    torch.cuda.empty_cache()
+    c2 = sift_like(10_000_000, seed=2, n_components=4096, zipf=1.1, device=dev)
+    _, s2 = timed_build(c2, 10, 6, 3)
+    out["config2"] = {
+        "workload": "build: 10M SIFT-like descriptors (4,096-component mixture, Zipf(1.1) weights), B=10, L=6 "
+                    "(1M words), k-means++ init, 10 Lloyd iterations",
+        "value": s2, "unit": "s", "higher_is_better": False,
+        "note": "the reference supports B=16 only and cannot run this configuration",
+    }
+    del c2
+    torch.cuda.empty_cache()
+    return out
 
 
 SERVING_WORKLOAD = ("serving: 1M-word tree (B=10, L=6) trained on 10M SIFT-like descriptors from a 4,096-component "
