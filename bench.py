@@ -444,7 +444,7 @@ def scoring_bench(args, voc, dev, world, rank):
         "top_k": k, "value": world * nq / (ms / 1e3), "unit": "queries/s", "ms_per_batch": ms,
         "index_build_ms": index_ms, "first_batch_wall_ms": first_s * 1e3,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_kind,
+                     "frac": achieved / hbm_peak, "traffic": score_traffic(n_docs), "peak_source": peak_kind,
                      "kernel": "queryPrepKernel + scoreKernel", "launch_ms": kern_ms,
                      "algorithmic_bytes_per_launch": alg_bytes, "posting_pairs_read": pairs_read},
         "e2e": {"value": world * nq / e_s, "unit": "queries/s", "h2d_bytes_per_step": int(q_host.numel()) * 4,
@@ -614,6 +614,17 @@ def serving_bench(args, dev, rank):
             "db_postings": int(sizes.sum()), "gpu_event_ms_by_kernel": kernels,
             "note": "latency = submit to result on the host, including the host-to-device copy of the descriptors; "
                     "kernel times are event spans on streams that share the GPU"}
+
+
+def score_traffic(n_docs):
+    """DRAM bytes of one scoring launch from the ncu capture summarised in
+    profiles/score_kernel_c3.md (same seeded 20,000-image workload); None for other sizes."""
+    prof = os.path.join(ROOT, "profiles", "score_kernel_c3.md")
+    if n_docs != 20000 or not os.path.exists(prof):
+        return None
+    with open(prof) as fh:
+        m = re.search(r"^traffic_bytes_per_launch:\s*([0-9.]+)", fh.read(), re.M)
+    return float(m.group(1)) if m else None
 
 
 def scoring_cpu_baseline(voc, ids, doc_leaves, offs, queries, k, got_docs, got_counts, seconds):
