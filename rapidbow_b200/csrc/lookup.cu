@@ -33,20 +33,16 @@ constexpr uint32_t kTileRows = 128;
 constexpr uint32_t kTileBytes = kTileRows * kDims;    // 16 KB
 constexpr uint32_t kNodeBytes = kMaxBranch * kDims;   // 2 KB: one node's 16 centers
 constexpr uint32_t kBBlockBytes = kNodeBytes * 17;    // node + up to 16 children
-constexpr uint32_t kEpiWarpsPerRole = 4;              // one warp per TMEM lane quarter
-constexpr uint32_t kTcThreads = 32 * (2 + 2 * kEpiWarpsPerRole); // TMA, MMA, 4 A warps, 4 B warps
+constexpr uint32_t kTeamWarps = 4;                    // epilogue team: one warp per TMEM lane quarter
+constexpr uint32_t kTcThreads = 32 * (2 + 2 * kTeamWarps); // TMA, MMA, two epilogue teams
 constexpr uint32_t kSmemHistMax = 1024;
 // Two accumulator buffers of 256 columns; tile t uses buffer t & 1.  Its level-2p MMA (16
-// columns) lands in the first columns of the buffer and is read by the A warps before the
-// children MMA of the same tile overwrites the buffer.
+// columns) lands in the first columns of the buffer and is read by the buffer's epilogue team
+// before the children MMA of the same tile overwrites the buffer.
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kTmemBuf = 256;
 constexpr uint32_t kTileCache = 1024;
 constexpr uint32_t kGatherDepth = 4;                  // gathered tiles in flight (< kStages)
-// Branch hand-off ring between A and B warps.  The A warps write tile t + kBsSlots only after the
-// level-2p MMA of that tile, which waits for the B warps to release buffer (t + kBsSlots) & 1,
-// i.e. to finish tile t + 2 -- so 4 slots never overwrite a tile the B warps still read.
-constexpr uint32_t kBsSlots = 4;
 
 struct TcSmem {
     uint8_t a[kStages][kTileBytes];
@@ -56,10 +52,10 @@ struct TcSmem {
     uint64_t bFull[2];
     uint64_t bEmpty[2];
     uint64_t accA[2];     // level-2p MMA into buffer j complete (one phase per use of j)
-    uint64_t aRead[2];    // A warps have read the level-2p accumulators of buffer j
+    uint64_t aRead[2];    // team j has read the level-2p accumulators of buffer j
     uint64_t accB[2];     // children MMA into buffer j complete
     uint64_t bufFree[2];  // the last reader of buffer j is done with it
-    uint64_t bsReady[kBsSlots]; // A warps wrote the branches of tile t into bstar[t % kBsSlots]
+    uint64_t lowFree[2];  // team j has read columns [0, 128) of buffer j (two levels only)
     uint64_t mmaDone;
     uint32_t tmemBase;
     uint32_t abortFlag;
@@ -67,7 +63,6 @@ struct TcSmem {
     uint32_t hist[kSmemHistMax];
     TileInfo tileCache[kTileCache];    // this CTA's tile list (passes after the first)
     alignas(16) int32_t idx[kGatherDepth][kTileRows]; // gather row indices, ring
-    uint8_t bstar[kBsSlots][kTileRows];             // level-2p branch per row, A -> B warps
 };
 constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 1024;
 
@@ -112,17 +107,18 @@ __device__ __forceinline__ void tmemWaitTie(uint32_t (&r)[16])
                  :
                  : "memory");
 }
-// 32 lanes x 128 columns of 32-bit accumulators.
-__device__ __forceinline__ void tmemLoad128(uint32_t taddr, uint32_t (&r)[128])
+
+// 32 lanes x 64 columns of 32-bit accumulators, and the wait that ties them.
+__device__ __forceinline__ void tmemLoad64(uint32_t taddr, uint32_t (&r)[64])
 {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x128.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63, %64, %65, %66, %67, %68, %69, %70, %71, %72, %73, %74, %75, %76, %77, %78, %79, %80, %81, %82, %83, %84, %85, %86, %87, %88, %89, %90, %91, %92, %93, %94, %95, %96, %97, %98, %99, %100, %101, %102, %103, %104, %105, %106, %107, %108, %109, %110, %111, %112, %113, %114, %115, %116, %117, %118, %119, %120, %121, %122, %123, %124, %125, %126, %127}, [%128];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63]), "=r"(r[64]), "=r"(r[65]), "=r"(r[66]), "=r"(r[67]), "=r"(r[68]), "=r"(r[69]), "=r"(r[70]), "=r"(r[71]), "=r"(r[72]), "=r"(r[73]), "=r"(r[74]), "=r"(r[75]), "=r"(r[76]), "=r"(r[77]), "=r"(r[78]), "=r"(r[79]), "=r"(r[80]), "=r"(r[81]), "=r"(r[82]), "=r"(r[83]), "=r"(r[84]), "=r"(r[85]), "=r"(r[86]), "=r"(r[87]), "=r"(r[88]), "=r"(r[89]), "=r"(r[90]), "=r"(r[91]), "=r"(r[92]), "=r"(r[93]), "=r"(r[94]), "=r"(r[95]), "=r"(r[96]), "=r"(r[97]), "=r"(r[98]), "=r"(r[99]), "=r"(r[100]), "=r"(r[101]), "=r"(r[102]), "=r"(r[103]), "=r"(r[104]), "=r"(r[105]), "=r"(r[106]), "=r"(r[107]), "=r"(r[108]), "=r"(r[109]), "=r"(r[110]), "=r"(r[111]), "=r"(r[112]), "=r"(r[113]), "=r"(r[114]), "=r"(r[115]), "=r"(r[116]), "=r"(r[117]), "=r"(r[118]), "=r"(r[119]), "=r"(r[120]), "=r"(r[121]), "=r"(r[122]), "=r"(r[123]), "=r"(r[124]), "=r"(r[125]), "=r"(r[126]), "=r"(r[127])
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
                  : "r"(taddr));
 }
-__device__ __forceinline__ void tmemWaitTie128(uint32_t (&r)[128])
+__device__ __forceinline__ void tmemWaitTie64(uint32_t (&r)[64])
 {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31]), "+r"(r[32]), "+r"(r[33]), "+r"(r[34]), "+r"(r[35]), "+r"(r[36]), "+r"(r[37]), "+r"(r[38]), "+r"(r[39]), "+r"(r[40]), "+r"(r[41]), "+r"(r[42]), "+r"(r[43]), "+r"(r[44]), "+r"(r[45]), "+r"(r[46]), "+r"(r[47]), "+r"(r[48]), "+r"(r[49]), "+r"(r[50]), "+r"(r[51]), "+r"(r[52]), "+r"(r[53]), "+r"(r[54]), "+r"(r[55]), "+r"(r[56]), "+r"(r[57]), "+r"(r[58]), "+r"(r[59]), "+r"(r[60]), "+r"(r[61]), "+r"(r[62]), "+r"(r[63]), "+r"(r[64]), "+r"(r[65]), "+r"(r[66]), "+r"(r[67]), "+r"(r[68]), "+r"(r[69]), "+r"(r[70]), "+r"(r[71]), "+r"(r[72]), "+r"(r[73]), "+r"(r[74]), "+r"(r[75]), "+r"(r[76]), "+r"(r[77]), "+r"(r[78]), "+r"(r[79]), "+r"(r[80]), "+r"(r[81]), "+r"(r[82]), "+r"(r[83]), "+r"(r[84]), "+r"(r[85]), "+r"(r[86]), "+r"(r[87]), "+r"(r[88]), "+r"(r[89]), "+r"(r[90]), "+r"(r[91]), "+r"(r[92]), "+r"(r[93]), "+r"(r[94]), "+r"(r[95]), "+r"(r[96]), "+r"(r[97]), "+r"(r[98]), "+r"(r[99]), "+r"(r[100]), "+r"(r[101]), "+r"(r[102]), "+r"(r[103]), "+r"(r[104]), "+r"(r[105]), "+r"(r[106]), "+r"(r[107]), "+r"(r[108]), "+r"(r[109]), "+r"(r[110]), "+r"(r[111]), "+r"(r[112]), "+r"(r[113]), "+r"(r[114]), "+r"(r[115]), "+r"(r[116]), "+r"(r[117]), "+r"(r[118]), "+r"(r[119]), "+r"(r[120]), "+r"(r[121]), "+r"(r[122]), "+r"(r[123]), "+r"(r[124]), "+r"(r[125]), "+r"(r[126]), "+r"(r[127])
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31]), "+r"(r[32]), "+r"(r[33]), "+r"(r[34]), "+r"(r[35]), "+r"(r[36]), "+r"(r[37]), "+r"(r[38]), "+r"(r[39]), "+r"(r[40]), "+r"(r[41]), "+r"(r[42]), "+r"(r[43]), "+r"(r[44]), "+r"(r[45]), "+r"(r[46]), "+r"(r[47]), "+r"(r[48]), "+r"(r[49]), "+r"(r[50]), "+r"(r[51]), "+r"(r[52]), "+r"(r[53]), "+r"(r[54]), "+r"(r[55]), "+r"(r[56]), "+r"(r[57]), "+r"(r[58]), "+r"(r[59]), "+r"(r[60]), "+r"(r[61]), "+r"(r[62]), "+r"(r[63])
                  :
                  : "memory");
 }
@@ -205,13 +201,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         for (uint32_t j = 0; j < 2; j++) {
             mbarInit(&S.bFull[j], 1);
-            mbarInit(&S.bEmpty[j], 1 + (two ? 2u : 1u) * kEpiWarpsPerRole); // MMA commit + epilogue warps
+            mbarInit(&S.bEmpty[j], 1 + 2 * kTeamWarps); // MMA commit + both epilogue teams
             mbarInit(&S.accA[j], 1);
-            mbarInit(&S.aRead[j], kEpiWarpsPerRole);
+            mbarInit(&S.aRead[j], kTeamWarps);
             mbarInit(&S.accB[j], 1);
-            mbarInit(&S.bufFree[j], kEpiWarpsPerRole);
+            mbarInit(&S.bufFree[j], kTeamWarps);
+            mbarInit(&S.lowFree[j], kTeamWarps);
         }
-        for (uint32_t j = 0; j < kBsSlots; j++) mbarInit(&S.bsReady[j], kEpiWarpsPerRole);
         mbarInit(&S.mmaDone, 1);
         S.abortFlag = 0;
         fenceMbarInit();
@@ -346,10 +342,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     } else if (nT > 0 && warp == 1) {
         // ------------------------------------------------------------ MMA issuer (one thread)
         // Tile t accumulates in TMEM buffer j = t & 1 (columns [256 j, 256 j + 256)).  Tiles go
-        // in pairs: a(t) a(t+1) b(t) b(t+1) a(t+2) ...  a(t) (level 2p, 16 columns) needs the
-        // buffer released by the readers of tile t-2; b(t) (children, 16 B columns) overwrites
-        // the same buffer once the A warps have read a(t).  While the epilogue warps read one
-        // buffer the tensor pipe works on the other.  One level: a(t) only, in the same buffers.
+        // in pairs: a(t) a(t+1) b(t) b(t+1) a(t+2) ...  a(t) (level 2p, 16 columns) needs only
+        // the buffer's first 16 columns, which the epilogue team releases after the first
+        // 128-column load of tile t-2, so the level-2p MMA of tile t overlaps the rest of that
+        // read; b(t) (children, 16 B columns) waits for the whole buffer and for the team to have
+        // read a(t).  One level: a(t) only, released after the team's read.
         // (Issuing out of this order, b(t) as soon as a(t) was read, measured slower.)
         if (lane == 0) {
             const uint32_t idescA = idescU8(16);
@@ -369,7 +366,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
                 slotOf[j] = slot;
                 if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21)) return false;
-                if (t >= 2 && !mbarWait(&S.bufFree[j], ((t >> 1) - 1u) & 1u, abortFlag, p.err, 22)) return false;
+                if (t >= 2 && !mbarWait(two ? &S.lowFree[j] : &S.bufFree[j], ((t >> 1) - 1u) & 1u, abortFlag,
+                                        p.err, 22))
+                    return false;
                 tcFenceAfter();
                 const uint32_t aBase = smemAddr(S.a[s]);
                 const uint32_t bBase = smemAddr(S.b[slot]);
@@ -390,6 +389,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const uint32_t s = t % kStages;
                 const uint32_t sl = slotOf[j];
                 if (!mbarWait(&S.aRead[j], (t >> 1) & 1u, abortFlag, p.err, 23)) return false;
+                if (t >= 2 && !mbarWait(&S.bufFree[j], ((t >> 1) - 1u) & 1u, abortFlag, p.err, 25)) return false;
                 tcFenceAfter();
                 const uint32_t aBase = smemAddr(S.a[s]);
                 const uint32_t bBase = smemAddr(S.b[sl]) + kNodeBytes;
@@ -413,12 +413,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mbarWait(&S.mmaDone, 0, abortFlag, p.err, 24);
         }
         __syncwarp();
-    } else if (nT > 0 && warp >= 2 && warp < 2 + kEpiWarpsPerRole) {
-        // ------------------------------------------------------------ A warps: level-2p argmin
-        // One warp per TMEM lane quarter; each thread owns one tile row.  With two levels the
-        // branch is handed to the B warps through shared memory (written before the arrival
-        // the B warps wait on), and the buffer goes on to the children MMA; with one level the
-        // A warps are its last readers.
+    } else if (nT > 0 && warp >= 2) {
+        // ------------------------------------------------------------ epilogue teams
+        // Team j (warps 2 + 4 j .. 5 + 4 j, one per TMEM lane quarter; each thread owns one tile
+        // row) serves buffer j: the tiles t with t & 1 == j.  Per tile it reads the level-2p
+        // accumulators and picks the branch (releasing them to the children MMA), then reads the
+        // row's 16 * B children columns in 64-column loads -- releasing the first 128
+        // columns, where the next level-2p MMA of the buffer lands, after the first load and the
+        // buffer after the second -- and keeps the 16 columns of the chosen child.  The branch
+        // stays in a register.  With one level the team releases the buffer after the level-2p
+        // read.  Each team passes every tile so that both arrive once per centre group on bEmpty.
+        const uint32_t team = (warp - 2u) / kTeamWarps;
         const uint32_t q = warp & 3u;
         const uint32_t row = q * 32u + lane;
         const uint32_t tRow = tmem + ((q * 32u) << 16);
@@ -430,81 +435,59 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 slot ^= 1u;
                 prevGroup = ti.group;
             }
-            const uint32_t orig = (!two && row < ti.count) ? (gather ? __ldg(p.perm + ti.start + row) : ti.start + row) : 0u;
-            if (!mbarWait(&S.accA[j], (t >> 1) & 1u, abortFlag, p.err, 30)) break;
-            tcFenceAfter();
-            uint32_t r[16];
-            tmemLoad16(tRow + kTmemBuf * j, r);
-            tmemWaitTie(r);
-            const uint32_t b = argminScores(r, &S.cn[slot][0][0]);
-            if (two) S.bstar[t % kBsSlots][row] = static_cast<uint8_t>(b);
-            tcFenceBefore();
-            __syncwarp();
-            if (lane == 0) {
-                if (two) {
-                    mbarArrive(&S.aRead[j]);
-                    mbarArrive(&S.bsReady[t % kBsSlots]);
-                } else {
-                    mbarArrive(&S.bufFree[j]);
-                }
-            }
-            if (!two && row < ti.count) emitRow(S, p, smemHist, orig, ti.group * p.B + b);
-            if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) {
-                __syncwarp();
-                if (lane == 0) mbarArrive(&S.bEmpty[slot]);
-            }
-        }
-    } else if (nT > 0 && two && warp >= 2 + kEpiWarpsPerRole) {
-        // ------------------------------------------------------------ B warps: level-(2p+1) argmin
-        // Each thread reads its row's 16 * B children columns (two 128-column loads), releases the
-        // buffer, and keeps the 16 columns of the child its A warp chose.
-        const uint32_t q = warp & 3u;
-        const uint32_t row = q * 32u + lane;
-        const uint32_t tRow = tmem + ((q * 32u) << 16);
-        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1;
-        for (uint32_t t = 0; t < nT; t++) {
-            const uint32_t j = t & 1u;
-            const TileInfo ti = tileAtSmem(S, p, t0, t);
-            if (ti.group != prevGroup) {
-                slot ^= 1u;
-                prevGroup = ti.group;
-            }
-            const uint32_t orig = row < ti.count ? (gather ? __ldg(p.perm + ti.start + row) : ti.start + row) : 0u;
-            if (!mbarWait(&S.accB[j], (t >> 1) & 1u, abortFlag, p.err, 31)) break;
-            // acquire the A warps' branch writes for this tile
-            if (!mbarWait(&S.bsReady[t % kBsSlots], (t / kBsSlots) & 1u, abortFlag, p.err, 32)) break;
-            tcFenceAfter();
-            const uint32_t bs = S.bstar[t % kBsSlots][row];
-            uint32_t sel[16];
-#pragma unroll
-            for (int i = 0; i < 16; i++) sel[i] = 0;
-            {
+            if (j == team) {
+                const uint32_t orig = row < ti.count ? (gather ? __ldg(p.perm + ti.start + row) : ti.start + row) : 0u;
                 const uint32_t base = tRow + kTmemBuf * j;
-                uint32_t r[128];
-                tmemLoad128(base, r);
-                tmemWaitTie128(r);
-                if (p.B > 8) {
-#pragma unroll
-                    for (uint32_t k = 0; k < 8; k++)
-#pragma unroll
-                        for (int i = 0; i < 16; i++) sel[i] = bs == k ? r[16 * k + i] : sel[i];
-                    tmemLoad128(base + 128u, r);
-                    tmemWaitTie128(r);
+                if (!mbarWait(&S.accA[j], (t >> 1) & 1u, abortFlag, p.err, 30)) break;
+                tcFenceAfter();
+                uint32_t b;
+                {
+                    uint32_t r[16];
+                    tmemLoad16(base, r);
+                    tmemWaitTie(r);
+                    b = argminScores(r, &S.cn[slot][0][0]);
                 }
-                // the accumulators are in registers: the buffer can take tile t + 2
                 tcFenceBefore();
                 __syncwarp();
-                if (lane == 0) mbarArrive(&S.bufFree[j]);
-                const uint32_t k0 = p.B > 8 ? 8u : 0u;
+                if (lane == 0) mbarArrive(two ? &S.aRead[j] : &S.bufFree[j]);
+                if (!two) {
+                    if (row < ti.count) emitRow(S, p, smemHist, orig, ti.group * p.B + b);
+                } else {
+                    if (!mbarWait(&S.accB[j], (t >> 1) & 1u, abortFlag, p.err, 31)) break;
+                    tcFenceAfter();
+                    uint32_t sel[16];
 #pragma unroll
-                for (uint32_t k = 0; k < 8; k++)
+                    for (int i = 0; i < 16; i++) sel[i] = 0;
+                    // children 4 h .. 4 h + 3 are columns [64 h, 64 h + 64)
+                    auto pick = [&](uint32_t h) {
+                        uint32_t r[64];
+                        tmemLoad64(base + 64u * h, r);
+                        tmemWaitTie64(r);
 #pragma unroll
-                    for (int i = 0; i < 16; i++) sel[i] = bs == k0 + k ? r[16 * k + i] : sel[i];
-            }
-            if (row < ti.count) {
-                const uint64_t child = uint64_t(ti.group) * p.B + bs; // in-level index at level 2p+1
-                const uint32_t b2 = argminScores(sel, &S.cn[slot][1 + bs][0]);
-                emitRow(S, p, smemHist, orig, static_cast<uint32_t>(child * p.B + b2));
+                        for (uint32_t k = 0; k < 4; k++)
+#pragma unroll
+                            for (int i = 0; i < 16; i++) sel[i] = b == 4 * h + k ? r[16 * k + i] : sel[i];
+                    };
+                    pick(0);
+                    pick(1);
+                    // columns [0, 128) have been read: the level-2p MMA of tile t + 2 may start
+                    tcFenceBefore();
+                    __syncwarp();
+                    if (lane == 0) mbarArrive(&S.lowFree[j]);
+                    if (p.B > 8) {
+                        pick(2);
+                        pick(3);
+                    }
+                    // the accumulators are in registers: the buffer can take tile t + 2
+                    tcFenceBefore();
+                    __syncwarp();
+                    if (lane == 0) mbarArrive(&S.bufFree[j]);
+                    if (row < ti.count) {
+                        const uint64_t child = uint64_t(ti.group) * p.B + b; // in-level index at level 2p+1
+                        const uint32_t b2 = argminScores(sel, &S.cn[slot][1 + b][0]);
+                        emitRow(S, p, smemHist, orig, static_cast<uint32_t>(child * p.B + b2));
+                    }
+                }
             }
             if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) {
                 __syncwarp();
