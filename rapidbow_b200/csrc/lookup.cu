@@ -34,7 +34,8 @@ constexpr uint32_t kTileBytes = kTileRows * kDims;    // 16 KB
 constexpr uint32_t kNodeBytes = kMaxBranch * kDims;   // 2 KB: one node's 16 centers
 constexpr uint32_t kBBlockBytes = kNodeBytes * 17;    // node + up to 16 children
 constexpr uint32_t kTeamWarps = 4;                    // epilogue team: one warp per TMEM lane quarter
-constexpr uint32_t kTcThreads = 32 * (2 + 2 * kTeamWarps); // TMA, MMA, two epilogue teams
+constexpr uint32_t kIssuer1Warp = 2 + 2 * kTeamWarps;        // second MMA issuer, after the teams
+constexpr uint32_t kTcThreads = 32 * (3 + 2 * kTeamWarps); // TMA, two MMA issuers, two epilogue teams
 constexpr uint32_t kSmemHistMax = 1024;
 // Two accumulator buffers of 256 columns; tile t uses buffer t & 1.  Its level-2p MMA (16
 // columns) lands in the first columns of the buffer and is read by the buffer's epilogue team
@@ -201,14 +202,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         for (uint32_t j = 0; j < 2; j++) {
             mbarInit(&S.bFull[j], 1);
-            mbarInit(&S.bEmpty[j], 1 + 2 * kTeamWarps); // MMA commit + both epilogue teams
+            mbarInit(&S.bEmpty[j], 2 + 2 * kTeamWarps); // both MMA issuers + both epilogue teams
             mbarInit(&S.accA[j], 1);
             mbarInit(&S.aRead[j], kTeamWarps);
             mbarInit(&S.accB[j], 1);
             mbarInit(&S.bufFree[j], kTeamWarps);
             mbarInit(&S.lowFree[j], kTeamWarps);
         }
-        mbarInit(&S.mmaDone, 1);
+        mbarInit(&S.mmaDone, 2);
         S.abortFlag = 0;
         fenceMbarInit();
     }
@@ -339,81 +340,68 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
         }
         __syncwarp();
-    } else if (nT > 0 && warp == 1) {
-        // ------------------------------------------------------------ MMA issuer (one thread)
-        // Tile t accumulates in TMEM buffer j = t & 1 (columns [256 j, 256 j + 256)).  Tiles go
-        // in pairs: a(t) a(t+1) b(t) b(t+1) a(t+2) ...  a(t) (level 2p, 16 columns) needs only
-        // the buffer's first 16 columns, which the epilogue team releases after the first
-        // 128-column load of tile t-2, so the level-2p MMA of tile t overlaps the rest of that
-        // read; b(t) (children, 16 B columns) waits for the whole buffer and for the team to have
-        // read a(t).  One level: a(t) only, released after the team's read.
-        // (Issuing out of this order, b(t) as soon as a(t) was read, measured slower.)
+    } else if (nT > 0 && (warp == 1 || warp == kIssuer1Warp)) {
+        // ------------------------------------------------------------ MMA issuers (one thread each)
+        // Issuer j (warp 1 for j = 0, warp kIssuer1Warp for j = 1) issues the MMAs of the tiles
+        // t with t & 1 == j, which accumulate in TMEM buffer j (columns [256 j, 256 j + 256)):
+        // a(t) (level 2p, 16 columns) needs only the buffer's first 16 columns, which epilogue
+        // team j releases after the first 128-column load of tile t-2, so the level-2p MMA of
+        // tile t overlaps the rest of that read; b(t) (children, 16 B columns) waits for the
+        // whole buffer and for the team to have read a(t).  One level: a(t) only, released after
+        // the team's read.  Two issuers let one buffer's MMAs go while the other's thread
+        // waits; commits track only the committing thread's MMAs, so each buffer's barriers see
+        // exactly its own tiles.  Both issuers pass every tile and commit once per centre group
+        // on the producer's "centre block free" barrier.
         if (lane == 0) {
+            const uint32_t jm = warp == 1 ? 0u : 1u;
             const uint32_t idescA = idescU8(16);
             const uint32_t idescB = idescU8(16 * p.B);
             uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, uses0 = 0, uses1 = 0;
-            uint32_t slotOf[2] = {0, 0};
             bool ok = true;
-            auto issueA = [&](uint32_t t) -> bool {
-                const uint32_t j = t & 1u;
-                const uint32_t s = t % kStages;
+            for (uint32_t t = 0; ok && t < nT; t++) {
                 const TileInfo ti = tileAtSmem(S, p, t0, t);
                 if (ti.group != prevGroup) {
                     slot ^= 1u;
                     const uint32_t u = slot ? uses1++ : uses0++;
-                    if (!mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 20)) return false;
+                    if (!mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 20)) break;
                     prevGroup = ti.group;
                 }
-                slotOf[j] = slot;
-                if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21)) return false;
-                if (t >= 2 && !mbarWait(two ? &S.lowFree[j] : &S.bufFree[j], ((t >> 1) - 1u) & 1u, abortFlag,
-                                        p.err, 22))
-                    return false;
-                tcFenceAfter();
-                const uint32_t aBase = smemAddr(S.a[s]);
-                const uint32_t bBase = smemAddr(S.b[slot]);
+                if ((t & 1u) == jm) {
+                    const uint32_t j = jm;
+                    const uint32_t s = t % kStages;
+                    if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21)) break;
+                    if (t >= 2 && !mbarWait(two ? &S.lowFree[j] : &S.bufFree[j], ((t >> 1) - 1u) & 1u, abortFlag,
+                                            p.err, 22))
+                        break;
+                    tcFenceAfter();
+                    const uint32_t aBase = smemAddr(S.a[s]);
+                    const uint32_t bBase = smemAddr(S.b[slot]);
 #pragma unroll
-                for (uint32_t q4 = 0; q4 < 4; q4++) {
-                    mmaU8(tmem + kTmemBuf * j, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4),
-                          idescA, q4 > 0 ? 1u : 0u);
-                }
-                mmaCommit(&S.accA[j]);
-                if (!two) {
+                    for (uint32_t q4 = 0; q4 < 4; q4++) {
+                        mmaU8(tmem + kTmemBuf * j, smemDescSw128(aBase + 32u * q4),
+                              smemDescSw128(bBase + 32u * q4), idescA, q4 > 0 ? 1u : 0u);
+                    }
+                    mmaCommit(&S.accA[j]);
+                    if (two) {
+                        if (!mbarWait(&S.aRead[j], (t >> 1) & 1u, abortFlag, p.err, 23)) break;
+                        if (t >= 2 && !mbarWait(&S.bufFree[j], ((t >> 1) - 1u) & 1u, abortFlag, p.err, 25)) break;
+                        tcFenceAfter();
+#pragma unroll
+                        for (uint32_t q4 = 0; q4 < 4; q4++) {
+                            mmaU8(tmem + kTmemBuf * j, smemDescSw128(aBase + 32u * q4),
+                                  smemDescSw128(bBase + kNodeBytes + 32u * q4), idescB, q4 > 0 ? 1u : 0u);
+                        }
+                        mmaCommit(&S.accB[j]);
+                    }
                     mmaCommit(&S.aEmpty[s]);
-                    if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[slot]);
                 }
-                return true;
-            };
-            auto issueB = [&](uint32_t t) -> bool {
-                const uint32_t j = t & 1u;
-                const uint32_t s = t % kStages;
-                const uint32_t sl = slotOf[j];
-                if (!mbarWait(&S.aRead[j], (t >> 1) & 1u, abortFlag, p.err, 23)) return false;
-                if (t >= 2 && !mbarWait(&S.bufFree[j], ((t >> 1) - 1u) & 1u, abortFlag, p.err, 25)) return false;
-                tcFenceAfter();
-                const uint32_t aBase = smemAddr(S.a[s]);
-                const uint32_t bBase = smemAddr(S.b[sl]) + kNodeBytes;
-#pragma unroll
-                for (uint32_t q4 = 0; q4 < 4; q4++) {
-                    mmaU8(tmem + kTmemBuf * j, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4),
-                          idescB, q4 > 0 ? 1u : 0u);
-                }
-                mmaCommit(&S.accB[j]);
-                mmaCommit(&S.aEmpty[s]);
-                if (lastOfGroupSmem(S, p, t0, nT, t, tileAtSmem(S, p, t0, t).group)) mmaCommit(&S.bEmpty[sl]);
-                return true;
-            };
-            for (uint32_t t = 0; ok && t < nT; t += 2) {
-                ok = issueA(t);
-                if (ok && t + 1 < nT) ok = issueA(t + 1);
-                if (ok && two) ok = issueB(t);
-                if (ok && two && t + 1 < nT) ok = issueB(t + 1);
+                if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[slot]);
             }
             mmaCommit(&S.mmaDone);
             mbarWait(&S.mmaDone, 0, abortFlag, p.err, 24);
         }
         __syncwarp();
-    } else if (nT > 0 && warp >= 2) {
+    } else if (nT > 0 && warp >= 2 && warp < 2 + 2 * kTeamWarps) {
         // ------------------------------------------------------------ epilogue teams
         // Team j (warps 2 + 4 j .. 5 + 4 j, one per TMEM lane quarter; each thread owns one tile
         // row) serves buffer j: the tiles t with t & 1 == j.  Per tile it reads the level-2p
