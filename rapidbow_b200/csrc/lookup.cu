@@ -231,8 +231,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (nT > 0 && warp == 0) {
         // ------------------------------------------------------------ producer
         // First pass: one TMA tiled load (128 rows, 128-byte swizzle) per tile.
-        // Later passes: the tile's 128 rows are gathered with 16-byte cp.async (lane q copies rows
-        // 4q..4q+3, 8 chunks each) into the same swizzled layout, kGatherDepth tiles in flight.
+        // Later passes: the tile's 128 rows are gathered with 16-byte cp.async (lane q copies chunk
+        // q % 8 of rows 4k + q / 8) into the same swizzled layout, kGatherDepth tiles in flight.
         // Row indices travel through a shared-memory ring inside the same copy groups: group #i
         // (prologue for i < kGatherDepth, else committed by iteration i - kGatherDepth) carries
         // the indices of tile i and the rows of tile i - kGatherDepth, so wait_group(depth - 1)
@@ -311,16 +311,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (!gather) {
                 if (lane == 0) tmaLoad2d(S.a[s], &tmapTile, 0, static_cast<int32_t>(ti.start), &S.aFull[s]);
             } else {
-                const int4 rows = *reinterpret_cast<const int4*>(&S.idx[i % kGatherDepth][4 * lane]);
-                const uint32_t rowIdx[4] = {static_cast<uint32_t>(rows.x), static_cast<uint32_t>(rows.y),
-                                            static_cast<uint32_t>(rows.z), static_cast<uint32_t>(rows.w)};
+                // Eight consecutive lanes copy the eight 16-byte chunks of one row, so each
+                // instruction moves four whole 128-byte rows (4 lines, not 32).  The indices were
+                // written by other lanes' copies: the wait above plus this barrier make them visible.
+                __syncwarp();
+                // All indices are read before the first copy: the copies are ordered with shared
+                // memory accesses, so reads interleaved with them would each wait in turn.
+                const int32_t* ring = &S.idx[i % kGatherDepth][0];
+                const uint32_t c = lane & 7u;
+                uint32_t rowIdx[kTileRows / 4];
 #pragma unroll
-                for (uint32_t r = 0; r < 4; r++) {
-                    const uint32_t tr = 4 * lane + r; // row within the tile
-                    const uint8_t* src = p.desc + uint64_t(rowIdx[r]) * kDims;
-                    uint8_t* dst = S.a[s] + tr * kDims;
+                for (uint32_t k = 0; k < kTileRows / 4; k++) rowIdx[k] = static_cast<uint32_t>(ring[4u * k + (lane >> 3)]);
 #pragma unroll
-                    for (uint32_t c = 0; c < 8; c++) cpAsync16(dst + ((c ^ (tr & 7u)) << 4), src + (c << 4));
+                for (uint32_t k = 0; k < kTileRows / 4; k++) {
+                    const uint32_t tr = 4u * k + (lane >> 3); // row within the tile
+                    cpAsync16(S.a[s] + tr * kDims + ((c ^ (tr & 7u)) << 4), p.desc + uint64_t(rowIdx[k]) * kDims + (c << 4));
                 }
                 copyIdx(i + kGatherDepth);
                 cpAsyncCommit();
