@@ -44,6 +44,11 @@ constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kTmemBuf = 256;
 constexpr uint32_t kTileCache = 1024;
 constexpr uint32_t kGatherDepth = 4;                  // gathered tiles in flight (< kStages)
+// Row-index ring: iteration i reads slot i % kIdxSlots and queues the copy of tile i + kGatherDepth
+// into slot (i + kGatherDepth) % kIdxSlots, which was last read in iteration i - 1 (behind that
+// iteration's closing warp barrier).  With kGatherDepth slots the copy would target the slot
+// other lanes were still reading, and rows were occasionally gathered from a wrong index.
+constexpr uint32_t kIdxSlots = kGatherDepth + 1;
 
 struct TcSmem {
     uint8_t a[kStages][kTileBytes];
@@ -63,7 +68,7 @@ struct TcSmem {
     alignas(16) int32_t cn[2][17][16]; // |c|^2 of each B slot: row 0 = node, rows 1.. = children
     uint32_t hist[kSmemHistMax];
     TileInfo tileCache[kTileCache];    // this CTA's tile list (passes after the first)
-    alignas(16) int32_t idx[kGatherDepth][kTileRows]; // gather row indices, ring
+    alignas(16) int32_t idx[kIdxSlots][kTileRows];    // gather row indices, ring
 };
 constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 1024;
 
@@ -232,7 +237,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // ------------------------------------------------------------ producer
         // First pass: one TMA tiled load (128 rows, 128-byte swizzle) per tile.
         // Later passes: the tile's 128 rows are gathered with 16-byte cp.async (lane q copies chunk
-        // q % 8 of rows 4k + q / 8) into the same swizzled layout, kGatherDepth tiles in flight.
+        // q % 8 of rows 32 (q / 8) + k) into the same swizzled layout, kGatherDepth tiles in flight.
         // Row indices travel through a shared-memory ring inside the same copy groups: group #i
         // (prologue for i < kGatherDepth, else committed by iteration i - kGatherDepth) carries
         // the indices of tile i and the rows of tile i - kGatherDepth, so wait_group(depth - 1)
@@ -244,7 +249,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
                 for (uint32_t j = 0; j < 4; j++) {
                     const uint32_t rr = 4 * lane + j;
-                    cpAsync4(&S.idx[i % kGatherDepth][rr], p.perm + ti.start + (rr < ti.count ? rr : 0u));
+                    cpAsync4(&S.idx[i % kIdxSlots][rr], p.perm + ti.start + (rr < ti.count ? rr : 0u));
                 }
             }
         };
@@ -317,14 +322,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 __syncwarp();
                 // All indices are read before the first copy: the copies are ordered with shared
                 // memory accesses, so reads interleaved with them would each wait in turn.
-                const int32_t* ring = &S.idx[i % kGatherDepth][0];
+                // Lane group g = lane / 8 copies rows 32 g .. 32 g + 31, whose indices it reads
+                // with eight 16-byte loads.
+                const int32_t* ring = &S.idx[i % kIdxSlots][0];
                 const uint32_t c = lane & 7u;
                 uint32_t rowIdx[kTileRows / 4];
 #pragma unroll
-                for (uint32_t k = 0; k < kTileRows / 4; k++) rowIdx[k] = static_cast<uint32_t>(ring[4u * k + (lane >> 3)]);
+                for (uint32_t k = 0; k < kTileRows / 16; k++) {
+                    const int4 v = *reinterpret_cast<const int4*>(ring + 32u * (lane >> 3) + 4u * k);
+                    rowIdx[4 * k] = static_cast<uint32_t>(v.x);
+                    rowIdx[4 * k + 1] = static_cast<uint32_t>(v.y);
+                    rowIdx[4 * k + 2] = static_cast<uint32_t>(v.z);
+                    rowIdx[4 * k + 3] = static_cast<uint32_t>(v.w);
+                }
 #pragma unroll
                 for (uint32_t k = 0; k < kTileRows / 4; k++) {
-                    const uint32_t tr = 4u * k + (lane >> 3); // row within the tile
+                    const uint32_t tr = 32u * (lane >> 3) + k; // row within the tile
                     cpAsync16(S.a[s] + tr * kDims + ((c ^ (tr & 7u)) << 4), p.desc + uint64_t(rowIdx[k]) * kDims + (c << 4));
                 }
                 copyIdx(i + kGatherDepth);
@@ -420,12 +433,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint32_t q = warp & 3u;
         const uint32_t row = q * 32u + lane;
         const uint32_t tRow = tmem + ((q * 32u) << 16);
-        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1;
+        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, uses0 = 0, uses1 = 0;
         for (uint32_t t = 0; t < nT; t++) {
             const uint32_t j = t & 1u;
             const TileInfo ti = tileAtSmem(S, p, t0, t);
             if (ti.group != prevGroup) {
+                // Wait for the group's centre block even when this team has no tile in it: the
+                // team's arrival on bEmpty for this group must not come before the block was
+                // loaded, or it would count toward the slot's previous group and free that
+                // block while the other team still reads it.
                 slot ^= 1u;
+                const uint32_t u = slot ? uses1++ : uses0++;
+                if (!mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 33)) break;
                 prevGroup = ti.group;
             }
             if (j == team) {

@@ -120,3 +120,20 @@ def test_blob_extension_for_other_branch_factors():
     assert voc2.branch_factor == 10 and voc2.nb_levels == 3
     c, m, w = voc2.tree()
     assert np.array_equal(c, centers) and np.array_equal(w, weights)
+
+
+def test_lookup_repeated_large_batches_are_exact():
+    """Many centre groups per CTA in the gathered pass and a producer that runs ahead of the
+    MMA: the double-buffered centre blocks and the row-index ring are reused as fast as the
+    hardware allows.  Every repetition must equal the FP32 kernel exactly."""
+    from rapidbow_b200.synth import sift_like
+
+    train = sift_like(500_000, seed=21, device="cuda")
+    voc = rbw.build_vocabulary(train, 16, nb_doc=1000, nb_levels=4, init="kmeans++", seed=5, max_iterations=5)
+    desc = sift_like(8_000_000, seed=22, device="cuda")
+    want = voc.lookup(desc, algo="simt_f32")
+    for _ in range(4):
+        got = voc.lookup(desc, algo="tensor_u8")
+        torch.cuda.synchronize()
+        assert voc.device_errors() == (0, 0)
+        assert int((got != want).sum()) == 0
