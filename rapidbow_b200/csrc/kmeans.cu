@@ -1,5 +1,6 @@
 // Hierarchical k-means kernels.  Distances are exact integers: score_b = |c_b|^2 - 2 x.c_b with
-// x.c_b from dp4a (u8 x u8 -> u32), argmin with the lowest index on ties (kmeans.cu:131-135).
+// x.c_b from the tensor core (tcgen05.mma.kind::i8, u8 x u8 -> s32) in the assign step and from
+// dp4a in k-means++, argmin with the lowest index on ties (kmeans.cu:131-135).
 // Center sums are exact (u32 in shared memory, u64 in global memory).
 #include "kmeans.cuh"
 #include "timing.h"
@@ -313,30 +314,79 @@ __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint
 }
 
 // ------------------------------------------------------------------ assign
+// One step handles one 128-member tile of one node (the reference's DescTile groups,
+// kmeans.cu:62-211, on the tensor core):
+//   1. the members' rows are gathered into shared memory in the 128-byte swizzled K-major layout
+//      (eight threads per row), next to the node's 16 centers in the same layout;
+//   2. one thread issues four tcgen05.mma.kind::i8 (M = 128 members, N = 16 centers, K = 4 x 32
+//      dims, u8 x u8 -> s32, exact) into this CTA's TMEM columns;
+//   3. warp w reads the dot products of rows 32w..32w+31 (its TMEM lane quarter) and takes the
+//      argmin of |c_b|^2 - 2 x.c_b, lowest index on ties (kmeans.cu:131-135), updating the
+//      assignment, the per-center counts and the changed count;
+//   4. the same warp adds its rows into the node's per-CTA center sums: lane l owns dims
+//      4l..4l+3 and adds each row's four bytes with shared atomics, the sums stored
+//      dim-interleaved so that the 32 lanes hit 32 banks.
+// Counts and sums go to global memory when the CTA moves to another node.  Several CTAs per SM
+// overlap one another's gathers, MMAs and sums.
 constexpr uint32_t kAssignThreads = 128;
+constexpr uint32_t kAssignRows = 128;
+constexpr uint32_t kAssignTmemCols = 32; // the smallest allocation; the MMA writes 16 columns
+constexpr uint32_t kAssignCtasPerSm = 6; // by registers (<= 80) and shared memory; 192 TMEM columns
 
-__global__ void __launch_bounds__(kAssignThreads) assignKernel(KMeansLevel lv, const NodeTile* tiles,
-                                                               const uint32_t* nTilesDev)
+struct AssignSmem {
+    uint8_t tile[kAssignRows * kDims];   // member rows, 128-byte swizzle (1024-byte aligned)
+    uint8_t cen[kMaxBranch * kDims];     // node centers, same layout
+    uint32_t acc[kMaxBranch * kDims];    // center sums of the current node, see accIndex
+    int32_t cn[kMaxBranch];
+    uint32_t cnt[kMaxBranch];
+    uint8_t bsel[kAssignRows];
+    uint64_t mmaBar;
+    uint32_t tmemBase;
+    uint32_t chg;
+    uint32_t abortFlag;
+};
+constexpr size_t kAssignSmemBytes = sizeof(AssignSmem) + 1024;
+
+// Position of (center b, dim d = 4 l + k) in AssignSmem::acc: b * 128 + 32 k + l.
+__device__ __forceinline__ uint32_t accIndex(uint32_t b, uint32_t d)
 {
-    __shared__ uint4 cs[kMaxBranch][8];       // node centers
-    __shared__ int32_t cn[kMaxBranch];
-    __shared__ uint32_t acc[kMaxBranch][kDims + 4]; // per-CTA center sums (padded rows)
-    __shared__ uint32_t cnt[kMaxBranch];
-    __shared__ uint32_t chg;
+    return b * kDims + (d & 3u) * 32u + (d >> 2);
+}
+
+__global__ void __launch_bounds__(kAssignThreads, kAssignCtasPerSm) assignKernel(KMeansLevel lv, const NodeTile* tiles,
+                                                                  const uint32_t* nTilesDev)
+{
+    extern __shared__ uint8_t smemRaw[];
+    AssignSmem& S = *reinterpret_cast<AssignSmem*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+    const uint32_t tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
     const uint32_t T = *nTilesDev;
     const uint32_t t0 = static_cast<uint32_t>(uint64_t(T) * blockIdx.x / gridDim.x);
     const uint32_t t1 = static_cast<uint32_t>(uint64_t(T) * (blockIdx.x + 1) / gridDim.x);
-    const uint32_t tid = threadIdx.x;
-    uint32_t curNode = 0xFFFFFFFFu;
+    volatile uint32_t* abortFlag = &S.abortFlag;
+    if (tid == 0) {
+        mbarInit(&S.mmaBar, 1);
+        S.abortFlag = 0;
+        fenceMbarInit();
+    }
+    if (warp == 0) {
+        tmemAlloc(&S.tmemBase, kAssignTmemCols);
+        tmemRelinquish();
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tmem = S.tmemBase;
+    uint32_t curNode = 0xFFFFFFFFu, phase = 0;
     auto flush = [&]() {
         __syncthreads();
         if (curNode != 0xFFFFFFFFu) {
-            for (uint32_t i = tid; i < kMaxBranch * kDims; i += blockDim.x) {
-                const uint32_t v = acc[i / kDims][i % kDims];
-                if (v) atomicAdd(lv.sums + uint64_t(curNode) * kMaxBranch * kDims + i, (unsigned long long)v);
+            for (uint32_t i = tid; i < kMaxBranch * kDims; i += kAssignThreads) {
+                const uint32_t b = i / kDims, d = i % kDims;
+                const uint32_t v = S.acc[accIndex(b, d)];
+                if (v) atomicAdd(lv.sums + (uint64_t(curNode) * kMaxBranch + b) * kDims + d, (unsigned long long)v);
             }
-            if (tid < kMaxBranch && cnt[tid]) atomicAdd(lv.counts + uint64_t(curNode) * kMaxBranch + tid, cnt[tid]);
-            if (tid == 0 && chg) atomicAdd(lv.changed + curNode, chg);
+            if (tid < kMaxBranch && S.cnt[tid]) atomicAdd(lv.counts + uint64_t(curNode) * kMaxBranch + tid, S.cnt[tid]);
+            if (tid == 0 && S.chg) atomicAdd(lv.changed + curNode, S.chg);
         }
         __syncthreads();
     };
@@ -346,65 +396,93 @@ __global__ void __launch_bounds__(kAssignThreads) assignKernel(KMeansLevel lv, c
         if (ti.node != curNode) {
             flush();
             curNode = ti.node;
-            for (uint32_t i = tid; i < kMaxBranch * 8; i += blockDim.x)
-                (&cs[0][0])[i] = reinterpret_cast<const uint4*>(lv.centers + uint64_t(curNode) * kMaxBranch * kDims)[i];
+            {
+                // thread i copies chunk i % 8 of center i / 8 (16 centers x 8 chunks)
+                const uint32_t b = tid / 8, c = tid % 8;
+                const uint4 v = reinterpret_cast<const uint4*>(lv.centers + (uint64_t(curNode) * kMaxBranch + b) * kDims)[c];
+                *reinterpret_cast<uint4*>(S.cen + b * kDims + ((c ^ (b & 7u)) << 4)) = v;
+            }
             if (tid < kMaxBranch) {
-                cn[tid] = lv.cnorm[uint64_t(curNode) * kMaxBranch + tid];
-                cnt[tid] = 0;
+                S.cn[tid] = lv.cnorm[uint64_t(curNode) * kMaxBranch + tid];
+                S.cnt[tid] = 0;
             }
-            for (uint32_t i = tid; i < kMaxBranch * (kDims + 4); i += blockDim.x) (&acc[0][0])[i] = 0;
-            if (tid == 0) chg = 0;
-            __syncthreads();
+            for (uint32_t i = tid; i < kMaxBranch * kDims; i += kAssignThreads) S.acc[i] = 0;
+            if (tid == 0) S.chg = 0;
         }
-        if (tid < ti.count) {
-            const uint64_t at = uint64_t(ti.start) + tid;
-            const uint32_t d = lv.members[at];
-            uint4 x[8];
-            const uint4* xs = reinterpret_cast<const uint4*>(lv.desc + uint64_t(d) * kDims);
+        {
+            // eight threads per row, 16 rows per round; rows past the tile's count repeat its
+            // first member (their results are not used)
+            const uint32_t c = tid % 8;
+            uint32_t m[kAssignRows / 16];
 #pragma unroll
-            for (int k = 0; k < 8; k++) x[k] = __ldg(xs + k);
-            int32_t best = 0;
-            uint32_t bi = 0;
-            for (uint32_t b = 0; b < kMaxBranch; b++) {
-                uint32_t dot = 0;
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const uint4 c = cs[b][k];
-                    dot = __dp4a(x[k].x, c.x, dot);
-                    dot = __dp4a(x[k].y, c.y, dot);
-                    dot = __dp4a(x[k].z, c.z, dot);
-                    dot = __dp4a(x[k].w, c.w, dot);
-                }
-                const int32_t s = cn[b] - 2 * static_cast<int32_t>(dot);
-                if (b == 0 || s < best) {
-                    best = s;
-                    bi = b;
-                }
+            for (uint32_t k = 0; k < kAssignRows / 16; k++) {
+                const uint32_t row = 16u * k + tid / 8;
+                m[k] = lv.members[uint64_t(ti.start) + (row < ti.count ? row : 0u)];
             }
-            const uint8_t old = lv.assign[at];
-            if (old != bi) atomicAdd(&chg, 1u);
-            lv.assign[at] = static_cast<uint8_t>(bi);
-            atomicAdd(&cnt[bi], 1u);
-            // 128 shared-memory atomics per member; rows are padded to 132 words so members of
-            // different centers start on different banks.
-            uint32_t* a = &acc[bi][0];
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const uint32_t w4[4] = {x[k].x, x[k].y, x[k].z, x[k].w};
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const uint32_t v = w4[q];
-                    const int base = k * 16 + q * 4;
-                    atomicAdd(a + base + 0, v & 0xFFu);
-                    atomicAdd(a + base + 1, (v >> 8) & 0xFFu);
-                    atomicAdd(a + base + 2, (v >> 16) & 0xFFu);
-                    atomicAdd(a + base + 3, v >> 24);
-                }
+            for (uint32_t k = 0; k < kAssignRows / 16; k++) {
+                const uint32_t row = 16u * k + tid / 8;
+                cpAsync16(S.tile + row * kDims + ((c ^ (row & 7u)) << 4), lv.desc + uint64_t(m[k]) * kDims + (c << 4));
             }
+            cpAsyncCommit();
+            cpAsyncWait<0>();
         }
+        // the copies and the center stores are generic-proxy writes read by the tensor core
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        if (tid == 0) {
+            tcFenceAfter();
+            const uint32_t aBase = smemAddr(S.tile), bBase = smemAddr(S.cen);
+#pragma unroll
+            for (uint32_t q4 = 0; q4 < 4; q4++)
+                mmaU8(tmem, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4), idescU8(16),
+                      q4 > 0 ? 1u : 0u);
+            mmaCommit(&S.mmaBar);
+        }
+        if (!mbarWait(&S.mmaBar, phase, abortFlag, lv.err, 40)) break;
+        phase ^= 1u;
+        tcFenceAfter();
+        const uint32_t row = tid; // warp w reads TMEM lanes 32w .. 32w + 31
+        uint32_t r[16];
+        tmemLoad16(tmem + ((warp * 32u) << 16), r);
+        tmemWaitTie(r);
+        tcFenceBefore(); // the next step's MMA overwrites these columns after the barriers below
+        int32_t best = S.cn[0] - 2 * static_cast<int32_t>(r[0]);
+        uint32_t bi = 0;
+#pragma unroll
+        for (uint32_t b = 1; b < kMaxBranch; b++) {
+            const int32_t sc = S.cn[b] - 2 * static_cast<int32_t>(r[b]);
+            if (sc < best) {
+                best = sc;
+                bi = b;
+            }
+        }
+        if (row < ti.count) {
+            const uint64_t at = uint64_t(ti.start) + row;
+            if (lv.assign[at] != bi) atomicAdd(&S.chg, 1u);
+            lv.assign[at] = static_cast<uint8_t>(bi);
+            atomicAdd(&S.cnt[bi], 1u);
+        }
+        S.bsel[row] = static_cast<uint8_t>(bi);
+        __syncwarp();
+        const uint32_t rEnd = ti.count < 32u * warp + 32u ? ti.count : 32u * warp + 32u;
+        for (uint32_t rr = 32u * warp; rr < rEnd; rr++) {
+            const uint32_t b = S.bsel[rr];
+            const uint32_t x = *reinterpret_cast<const uint32_t*>(S.tile + rr * kDims + (((lane >> 2) ^ (rr & 7u)) << 4) +
+                                                                  ((lane & 3u) << 2));
+            uint32_t* a = S.acc + b * kDims + lane;
+            atomicAdd(a, x & 0xFFu);
+            atomicAdd(a + 32, (x >> 8) & 0xFFu);
+            atomicAdd(a + 64, (x >> 16) & 0xFFu);
+            atomicAdd(a + 96, x >> 24);
+        }
+        __syncthreads(); // the tile and bsel are rewritten by the next step
     }
     flush();
+    if (warp == 0) {
+        tcFenceAfter();
+        tmemDealloc(tmem, kAssignTmemCols);
+    }
 }
 
 // ------------------------------------------------------------------ regroup
@@ -539,9 +617,12 @@ void launchAssign(const KMeansLevel& lv, const NodeTile* tiles, const uint32_t* 
     int dev = 0, sms = 0;
     RBW_CUDA(cudaGetDevice(&dev));
     RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const uint32_t grid = std::max(1u, std::min<uint32_t>(maxTiles, static_cast<uint32_t>(sms) * 8));
+    // A fixed grid: the occupancy query gave one CTA per SM on some launches, 3-4x slower.
+    static_assert(kAssignCtasPerSm * kAssignTmemCols <= 512, "TMEM columns of the resident CTAs");
+    static_assert(kAssignCtasPerSm * kAssignSmemBytes <= 227 * 1024, "shared memory of the resident CTAs");
+    const uint32_t grid = std::max(1u, std::min<uint32_t>(maxTiles, static_cast<uint32_t>(sms) * kAssignCtasPerSm));
     ScopedKernelTimer timer(kTimedAssign, s);
-    assignKernel<<<grid, kAssignThreads, 0, s>>>(lv, tiles, nTilesDev);
+    assignKernel<<<grid, kAssignThreads, kAssignSmemBytes, s>>>(lv, tiles, nTilesDev);
     RBW_CUDA(cudaGetLastError());
 }
 

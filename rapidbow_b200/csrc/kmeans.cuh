@@ -31,6 +31,7 @@ struct KMeansLevel {
     uint32_t* lastChanged;      // [nbNodes] previous iteration (0 = frozen)
     uint32_t* activeCount;      // [1] nodes whose update ran in the last step
     uint32_t ieeeDivision;      // 0: the reference's fast division, 1: IEEE round-to-nearest
+    DeviceErrors* err;          // bounded-wait timeouts of the assign kernel
 };
 
 // Exclusive scan helpers (multi-block), tmp needs scanTempWords(n) words.

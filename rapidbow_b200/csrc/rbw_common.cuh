@@ -244,6 +244,17 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16])
         : "r"(taddr));
 }
 __device__ __forceinline__ void tmemWaitLoad() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// Waits until the tcgen05.ld results are in registers; the operands tie the 16 registers to
+// the wait so no use of them is scheduled before it.
+__device__ __forceinline__ void tmemWaitTie(uint32_t (&r)[16])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                   "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]),
+                   "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
+}
 
 // Shared-memory matrix descriptor for a K-major operand laid out in 128-byte swizzle atoms
 // (8 rows x 128 B, atoms stacked densely along M/N): SBO = 1024 B, LBO = 16 B (unused),

@@ -366,6 +366,7 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
         lv.lastChanged = lastChanged.as<uint32_t>();
         lv.activeCount = activeCount;
         lv.ieeeDivision = opts.ieeeDivision ? 1u : 0u;
+        lv.err = voc->mErrors.as<DeviceErrors>();
 
         // ---- initial centers
         if (opts.initMode == kInitReference) {
@@ -442,6 +443,9 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
     for (size_t i = 0; i < occ.size(); i++) voc->mWeights[i] = idfWeight(nbDoc, occ[i]);
     voc->finalizeDevice(stream);
     RBW_CUDA(cudaStreamSynchronize(stream));
+    const DeviceErrors e = voc->takeDeviceErrors();
+    if (e.code != 0)
+        throw Error(kTimeout, "a bounded device wait gave up during the build (site " + std::to_string(e.where) + ")");
     if (stats) {
         stats->levels = L;
         stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
