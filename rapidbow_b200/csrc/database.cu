@@ -438,8 +438,19 @@ __global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
             const uint32_t a = P.seg[s].leafOff[uint64_t(en.word) * span];
             const uint32_t b = P.seg[s].leafOff[(uint64_t(en.word) + 1) * span];
             if (leafLevel) {
-                // eight pairs per lane in flight
+                // sixteen pairs per lane in flight
                 uint32_t p = a + lane;
+                for (; p + 480 < b; p += 512) {
+                    uint64_t pr[16];
+#pragma unroll
+                    for (int u = 0; u < 16; u++) pr[u] = pairs[p + 32 * u];
+#pragma unroll
+                    for (int u = 0; u < 16; u++) {
+                        const uint32_t i = static_cast<uint32_t>(pr[u] >> 32) - docBeg;
+                        if (!kSharded || i < nLocal)
+                            addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
+                    }
+                }
                 for (; p + 224 < b; p += 256) {
                     uint64_t pr[8];
 #pragma unroll
