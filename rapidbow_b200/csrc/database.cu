@@ -91,15 +91,15 @@ __device__ void bitonicSortShared(T* keys, uint32_t nPow2)
 {
     for (uint32_t k = 2; k <= nPow2; k <<= 1) {
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < nPow2; i += blockDim.x) {
-                const uint32_t ixj = i ^ j;
-                if (ixj > i) {
-                    const bool up = (i & k) == 0;
-                    const T a = keys[i], b = keys[ixj];
-                    if ((a > b) == up) {
-                        keys[i] = b;
-                        keys[ixj] = a;
-                    }
+            // pair t compares i = (t with a zero bit inserted at j) with i + j
+            for (uint32_t t = threadIdx.x; t < nPow2 / 2; t += blockDim.x) {
+                const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                const uint32_t ixj = i | j;
+                const bool up = (i & k) == 0;
+                const T a = keys[i], b = keys[ixj];
+                if ((a > b) == up) {
+                    keys[i] = b;
+                    keys[ixj] = a;
                 }
             }
             __syncthreads();
@@ -135,7 +135,7 @@ __device__ double l1NormWarp(const uint32_t* sorted, uint32_t n, const float* we
 {
     const uint32_t lane = threadIdx.x & 31u;
     double norm = 0;
-    uint64_t span = 1;
+    uint32_t span = 1; // B^it; leaf indices are 32-bit, so is every span
     for (uint32_t it = 0; it < L; it++) {
         const float* lw = weights + levelBegDev(B, L - 1 - it) * B;
         float next = lane < n ? lw[sorted[lane] / span] : 0.f;
@@ -264,16 +264,23 @@ __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* 
         const double norm = l1NormWarp(keys, n, weights, B, L);
         if (threadIdx.x == 0) qRcpF[q] = float(1 / norm); // DataBase.cpp:77-94
     }
-    uint64_t span = 1;
+    uint32_t span = 1; // B^it; leaf indices are 32-bit, so is every span
     const uint64_t limit = 16ull + 4ull * k; // DataBase.h:60-61, DataBase.cpp:125
     for (uint32_t it = 0; it < L; it++) {
         const uint32_t level = L - 1 - it;
         const uint64_t base = levelBegDev(B, level) * B;
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const uint32_t word = static_cast<uint32_t>(keys[i] / span);
+            const uint32_t word = keys[i] / span;
             if (i == 0 || keys[i - 1] / span != word) {
-                uint32_t run = 1;
-                while (i + run < n && keys[i + run] / span == word) run++;
+                // the run of `word` ends at the first key >= (word + 1) * span (keys are sorted)
+                const uint64_t end = (uint64_t(word) + 1) * span;
+                uint32_t lo = i + 1, hi = n;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (keys[mid] < end) lo = mid + 1;
+                    else hi = mid;
+                }
+                const uint32_t run = lo - i;
                 const uint64_t widx = base + word;
                 if (it == 0 || wordPost[widx] < limit) {
                     const uint32_t p = atomicAdd(&cnt, 1u);
