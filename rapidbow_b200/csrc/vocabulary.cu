@@ -297,6 +297,47 @@ uint32_t lookupHostPipelined(const Vocabulary& v, const uint8_t* hostDesc, uint6
     return kernels;
 }
 
+namespace {
+// Build scratch from the library's stream-ordered pool, allocated and freed on the build's
+// stream: repeated builds reuse the pool's memory instead of mapping it again, and freeing it
+// does not synchronise the device.
+class StreamBuffer
+{
+public:
+    StreamBuffer(size_t bytes, cudaStream_t s) : mStream{s}, mBytes{bytes}
+    {
+        if (bytes) RBW_CUDA(cudaMallocFromPoolAsync(&mPtr, bytes, libraryPool(), s));
+    }
+    StreamBuffer(const StreamBuffer&) = delete;
+    StreamBuffer& operator=(const StreamBuffer&) = delete;
+    StreamBuffer(StreamBuffer&& o) noexcept : mPtr{o.mPtr}, mStream{o.mStream}, mBytes{o.mBytes}
+    {
+        o.mPtr = nullptr;
+        o.mBytes = 0;
+    }
+    StreamBuffer& operator=(StreamBuffer&& o) noexcept
+    {
+        std::swap(mPtr, o.mPtr);
+        std::swap(mStream, o.mStream);
+        std::swap(mBytes, o.mBytes);
+        return *this;
+    }
+    ~StreamBuffer()
+    {
+        if (mPtr) cudaFreeAsync(mPtr, mStream);
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(mPtr); }
+    void* get() const { return mPtr; }
+    size_t bytes() const { return mBytes; }
+
+private:
+    void* mPtr = nullptr;
+    cudaStream_t mStream = nullptr;
+    size_t mBytes = 0;
+};
+} // namespace
+
 std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint8_t* devDesc, uint32_t nbDesc,
                                               uint32_t nbDoc, const BuildOptions& opts, cudaStream_t stream,
                                               BuildStats* stats)
@@ -318,16 +359,17 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
     const uint32_t maxTiles128 = static_cast<uint32_t>(n / 128 + maxLevelNodes + 1);
     const uint32_t maxTiles32 = static_cast<uint32_t>(n / 32 + maxLevelNodes + 1);
 
-    DeviceBuffer members(n * 4), members2(n * 4), assign(n);
-    DeviceBuffer nodeCnt(std::max<uint64_t>(maxChildNodes, 1) * 4), nodeOff(std::max<uint64_t>(maxChildNodes, 1) * 4);
-    DeviceBuffer childCnt(maxChildNodes * 4), childOff(maxChildNodes * 4);
-    DeviceBuffer counts(maxLevelNodes * kMaxBranch * 4), sums(maxLevelNodes * kMaxBranch * kDims * 8);
-    DeviceBuffer changed(maxLevelNodes * 4), lastChanged(maxLevelNodes * 4), small(64);
-    DeviceBuffer picks(maxLevelNodes * B * 4), nValid(maxLevelNodes * 4);
-    DeviceBuffer tiles128(uint64_t(maxTiles128) * sizeof(NodeTile)), tiles32(uint64_t(maxTiles32) * sizeof(NodeTile));
-    DeviceBuffer tileOff(maxLevelNodes * 4);
-    DeviceBuffer scanTmp(scanTempWords(std::max<uint64_t>(uint64_t(B) * maxTiles32, maxLevelNodes)) * 4);
-    DeviceBuffer tileHist(uint64_t(B) * maxTiles32 * 4), tileScan(uint64_t(B) * maxTiles32 * 4);
+    const cudaStream_t st = stream;
+    StreamBuffer members(n * 4, st), members2(n * 4, st), assign(n, st);
+    StreamBuffer nodeCnt(std::max<uint64_t>(maxChildNodes, 1) * 4, st), nodeOff(std::max<uint64_t>(maxChildNodes, 1) * 4, st);
+    StreamBuffer childCnt(maxChildNodes * 4, st), childOff(maxChildNodes * 4, st);
+    StreamBuffer counts(maxLevelNodes * kMaxBranch * 4, st), sums(maxLevelNodes * kMaxBranch * kDims * 8, st);
+    StreamBuffer changed(maxLevelNodes * 4, st), lastChanged(maxLevelNodes * 4, st), small(64, st);
+    StreamBuffer picks(maxLevelNodes * B * 4, st), nValid(maxLevelNodes * 4, st);
+    StreamBuffer tiles128(uint64_t(maxTiles128) * sizeof(NodeTile), st), tiles32(uint64_t(maxTiles32) * sizeof(NodeTile), st);
+    StreamBuffer tileOff(maxLevelNodes * 4, st);
+    StreamBuffer scanTmp(scanTempWords(std::max<uint64_t>(uint64_t(B) * maxTiles32, maxLevelNodes)) * 4, st);
+    StreamBuffer tileHist(uint64_t(B) * maxTiles32 * 4, st), tileScan(uint64_t(B) * maxTiles32 * 4, st);
     uint32_t* totals = small.as<uint32_t>();
     uint32_t* activeCount = small.as<uint32_t>() + 4;
 
