@@ -459,9 +459,9 @@ def scoring_bench(args, voc, dev, world, rank):
 
 
 def build_bench(args, dev, rank):
-    """Hierarchical k-means builds: config 0 (200,000 descriptors, B=16, L=3) with a CPU
-    baseline and an exactness check against the oracle, and config 2 (10M descriptors from a
-    4,096-component Zipf(1.1) mixture, B=10, L=6).  Both: seeded k-means++ init, 10 Lloyd
+    """Hierarchical k-means builds: 200,000 descriptors into a B=16, L=3 tree with a CPU
+    baseline and an exactness check against the oracle, and 10M descriptors from a
+    4,096-component Zipf(1.1) mixture into a B=10, L=6 tree.  Both: seeded k-means++ init, 10 Lloyd
     iterations.  The build API is synchronous; times are host wall clock around it."""
     import numpy as np
     import torch
@@ -490,7 +490,7 @@ def build_bench(args, dev, rank):
     rbw.timing_enable(False)
     assign_ms, _ = rbw.timing_read("kmeans_assign")
     update_ms, _ = rbw.timing_read("kmeans_update")
-    out["config0"] = {
+    out["b16_l3_200k"] = {
         "workload": "build: 200,000 SIFT-like descriptors, B=16, L=3 (4,096 words), k-means++ init, 10 Lloyd iterations",
         "value": s0, "unit": "s", "higher_is_better": False,
         # 1 warm-up + 5 timed builds recorded; nodes that converge early are skipped by the kernel
@@ -505,15 +505,15 @@ def build_bench(args, dev, rank):
         ref = Oracle().build_vocabulary(host, 1000, 16, 3, max_iter=10, init=INIT_KMEANSPP, seed=7)
         cpu_s = time.perf_counter() - t0
         centers, masks, weights = voc_ieee.tree()
-        out["config0"]["matches_oracle"] = bool(np.array_equal(centers, ref["centers"]) and
+        out["b16_l3_200k"]["matches_oracle"] = bool(np.array_equal(centers, ref["centers"]) and
                                                 np.array_equal(masks, ref["masks"]))
-        out["config0"]["cpu_baseline"] = {"value": cpu_s, "unit": "s", "cores": 1, "kind": "port",
+        out["b16_l3_200k"]["cpu_baseline"] = {"value": cpu_s, "unit": "s", "cores": 1, "kind": "port",
                                           "sample": "the same build (oracle restatement, one thread)"}
     del c0
     torch.cuda.empty_cache()
     c2 = sift_like(10_000_000, seed=2, n_components=4096, zipf=1.1, device=dev)
     _, s2 = timed_build(c2, 10, 6, 3)
-    out["config2"] = {
+    out["b10_l6_10m"] = {
         "workload": "build: 10M SIFT-like descriptors (4,096-component mixture, Zipf(1.1) weights), B=10, L=6 "
                     "(1M words), k-means++ init, 10 Lloyd iterations",
         "value": s2, "unit": "s", "higher_is_better": False,
@@ -618,8 +618,8 @@ def serving_bench(args, dev, rank):
 
 def score_traffic(n_docs):
     """DRAM bytes of one scoring launch from the ncu capture summarised in
-    profiles/score_kernel_c3.md (same seeded 20,000-image workload); None for other sizes."""
-    prof = os.path.join(ROOT, "profiles", "score_kernel_c3.md")
+    profiles/score_kernel_20k_images.md (same seeded 20,000-image workload); None for other sizes."""
+    prof = os.path.join(ROOT, "profiles", "score_kernel_20k_images.md")
     if n_docs != 20000 or not os.path.exists(prof):
         return None
     with open(prof) as fh:
