@@ -171,8 +171,7 @@ __device__ __forceinline__ void emitRow(TcSmem& S, const PassParams& p, bool sme
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-    lookupPassTc(const __grid_constant__ CUtensorMap tmapTile, const __grid_constant__ CUtensorMap tmapRow,
-                 const PassParams p)
+    lookupPassTc(const __grid_constant__ CUtensorMap tmapTile, const PassParams p)
 {
     extern __shared__ uint8_t smemRaw[];
     TcSmem& S = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
@@ -800,7 +799,6 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
                                       static_cast<int>(kTcSmemBytes)));
     });
     const CUtensorMap tmapTile = makeRowMap(desc, n, kTileRows);
-    const CUtensorMap tmapRow = makeRowMap(desc, n, 1);
     const uint32_t B = tree.B, L = tree.L;
     const uint32_t passes = (L + 1) / 2;
     const uint32_t grid = static_cast<uint32_t>(smCount());
@@ -842,7 +840,7 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
         }
         {
             ScopedKernelTimer timer(kTimedLookupPass, stream);
-            lookupPassTc<<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, tmapRow, p);
+            lookupPassTc<<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
             RBW_CUDA(cudaGetLastError());
         }
         kernels++;

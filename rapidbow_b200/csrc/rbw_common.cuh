@@ -155,22 +155,13 @@ __device__ __forceinline__ void cpAsyncWait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// TMA: 2D tiled load and 2D row gather (4 rows per instruction, box one row high).
+// TMA: 2D tiled load.
 __device__ __forceinline__ void tmaLoad2d(void* dst, const CUtensorMap* map, int32_t x, int32_t y, uint64_t* bar)
 {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%2, %3}], [%4];" ::"r"(smemAddr(dst)),
         "l"(map), "r"(x), "r"(y), "r"(smemAddr(bar))
-        : "memory");
-}
-__device__ __forceinline__ void tmaGather4(void* dst, const CUtensorMap* map, int32_t x, int32_t r0, int32_t r1,
-                                           int32_t r2, int32_t r3, uint64_t* bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smemAddr(dst)),
-        "l"(map), "r"(x), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(smemAddr(bar))
         : "memory");
 }
 // Untiled bulk copy global -> shared (16-B aligned addresses, size multiple of 16).
@@ -213,18 +204,6 @@ __device__ __forceinline__ void mmaU8(uint32_t dTmem, uint64_t aDesc, uint64_t b
         "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
         : "memory");
 }
-// D[tmem] (+)= A * B^T, bf16 x bf16 -> fp32.
-__device__ __forceinline__ void mmaBf16(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc,
-                                        uint32_t accumulate)
-{
-    const uint32_t z = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dTmem),
-        "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
-        : "memory");
-}
 // Arrive (once) on `bar` when all previously issued MMAs of this thread have completed.
 __device__ __forceinline__ void mmaCommit(uint64_t* bar)
 {
@@ -243,7 +222,6 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16])
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 }
-__device__ __forceinline__ void tmemWaitLoad() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 // Waits until the tcgen05.ld results are in registers; the operands tie the 16 registers to
 // the wait so no use of them is scheduled before it.
 __device__ __forceinline__ void tmemWaitTie(uint32_t (&r)[16])
@@ -271,7 +249,7 @@ __device__ __forceinline__ uint64_t smemDescSw128(uint32_t addr)
     return d;
 }
 
-// Instruction descriptors (M = 128, K-major A and B).
+// Instruction descriptor (M = 128, K-major A and B, uint8 x uint8 -> s32).
 __host__ __device__ constexpr uint32_t idescU8(uint32_t n)
 {
     return (2u << 4)              // D = S32
@@ -280,30 +258,7 @@ __host__ __device__ constexpr uint32_t idescU8(uint32_t n)
            | ((n >> 3) << 17)     // N
            | ((128u >> 4) << 24); // M
 }
-__host__ __device__ constexpr uint32_t idescBf16(uint32_t n)
-{
-    return (1u << 4)              // D = F32
-           | (1u << 7)            // A = BF16
-           | (1u << 10)           // B = BF16
-           | ((n >> 3) << 17) | ((128u >> 4) << 24);
-}
 
-__device__ __forceinline__ uint32_t laneId()
-{
-    uint32_t id;
-    asm("mov.u32 %0, %%laneid;" : "=r"(id));
-    return id;
-}
-__device__ __forceinline__ bool electOne()
-{
-    uint32_t pred = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t.reg .b32 r;\n\t"
-        "elect.sync r|p, 0xffffffff;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(pred));
-    return pred != 0;
-}
 #endif // __CUDACC__
 
 } // namespace rbw
