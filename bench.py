@@ -506,9 +506,9 @@ def build_bench(args, dev, rank):
         cpu_s = time.perf_counter() - t0
         centers, masks, weights = voc_ieee.tree()
         out["b16_l3_200k"]["matches_oracle"] = bool(np.array_equal(centers, ref["centers"]) and
-                                                np.array_equal(masks, ref["masks"]))
+                                                    np.array_equal(masks, ref["masks"]))
         out["b16_l3_200k"]["cpu_baseline"] = {"value": cpu_s, "unit": "s", "cores": 1, "kind": "port",
-                                          "sample": "the same build (oracle restatement, one thread)"}
+                                              "sample": "the same build (oracle restatement, one thread)"}
     del c0
     torch.cuda.empty_cache()
     c2 = sift_like(10_000_000, seed=2, n_components=4096, zipf=1.1, device=dev)
