@@ -7,15 +7,18 @@
 One step = one lookup of the rank's 10M descriptors (inputs resident in HBM, 1.28 GB > L2, so
 no flush is needed).  N > 1 runs one process per GPU (torchrun) with the tree replicated and
 10M descriptors per rank (weak scaling, no collective on the data path).  Rank 0 prints one
-JSON line.  The reference has no CPU lookup; `--impl reference` times the CPU restatement of
-its kernel (the oracle, all host threads) on the same workload shape.
+JSON line (the headline).  On one GPU the other workloads follow, one line each, prefixed with
+"# <name> " so that the headline stays the only JSON line: the vocabulary builds (200,000
+descriptors B=16 L=3; 10M descriptors B=10 L=6), batched inverted-file scoring (20,000 images)
+and serving (100,000 images, Poisson arrivals).  The reference has no CPU lookup;
+`--impl reference` times the CPU restatement of its kernel (the oracle, all host threads) on the
+same workload shape.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -31,6 +34,13 @@ B, L = 16, 4
 N_TRAIN = 2_000_000
 N_LOOKUP = 10_000_000
 BYTES_PER_DESC = 132  # 128 B read + 4 B leaf written (algorithmic, per descriptor per pass)
+# DRAM bytes per descriptor of one lookupPassTc launch: dram__bytes_read.sum + dram__bytes_write.sum
+# of an ncu capture of a 2M-descriptor lookup (B=16, L=4; both pass launches averaged).  Traffic
+# grows in proportion to the descriptors, so it is scaled to the timed launch.
+LOOKUP_PASS_DRAM_BYTES_PER_DESC = 136.6
+# DRAM bytes of one scoring launch (queryPrepKernel + scoreKernel) on the seeded 20,000-image
+# database with 256 queries, top-50, from an ncu capture of that workload.
+SCORE_DRAM_BYTES_20K_IMAGES = 1_582_356_000
 WORKLOAD = ("lookup of 10M fresh SIFT-like descriptors per GPU through a 65,536-word tree "
             "(B=16, L=4) trained on 2M descriptors (k-means++ init, 10 Lloyd iterations)")
 
@@ -48,11 +58,12 @@ def parse():
     p.add_argument("--no-scoring", action="store_true", help="skip the inverted-file scoring workload")
     p.add_argument("--db-docs", type=int, default=20000, help="images in the scoring database")
     p.add_argument("--no-build", action="store_true", help="skip the vocabulary-build workloads")
-    p.add_argument("--serving", action="store_true",
-                   help="also run the serving workload (1M-word tree, 100,000 images, Poisson arrivals)")
+    p.add_argument("--no-serving", action="store_true",
+                   help="skip the serving workload (1M-word tree, 100,000 images, Poisson arrivals)")
+    p.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own GPU lookup kernel")
     p.add_argument("--serving-docs", type=int, default=100_000)
     p.add_argument("--serving-rate", type=float, default=2000.0, help="arrivals per second")
-    p.add_argument("--serving-seconds", type=float, default=10.0)
+    p.add_argument("--serving-seconds", type=float, default=5.0)
     return p.parse_args()
 
 
@@ -269,16 +280,7 @@ def run_ours(args, world, rank, local):
     hbm_peak, peak_kind = peaks()
     k_avg_ms = k_ms / max(k_n, 1)
     achieved = n * BYTES_PER_DESC / (k_avg_ms / 1e3) / 1e9
-    # DRAM traffic of one pass launch: bytes per descriptor from the ncu capture summarised in
-    # profiles/lookup_pass_tc_2M.md (dram read + write of a 2M-descriptor launch; traffic grows
-    # in proportion to the descriptors), scaled to this launch.
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "lookup_pass_tc_2M.md")
-    if os.path.exists(prof):
-        with open(prof) as fh:
-            m = re.search(r"^traffic_bytes_per_descriptor:\s*([0-9.]+)", fh.read(), re.M)
-        if m:
-            traffic = float(m.group(1)) * n
+    traffic = LOOKUP_PASS_DRAM_BYTES_PER_DESC * n
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -291,7 +293,7 @@ def run_ours(args, world, rank, local):
         "bit_exact_vs_fp32_kernel": same,
         "refined_descriptors": 0,
         "fp32_simt": {"value": fp32_value, "unit": UNIT, "ms_per_step": ms_simt,
-                      "speedup": value / fp32_value},
+                      "speedup": value / fp32_value, "kernel": "lookupSimtF32"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
                      "kernel": "lookupPassTc", "launch_ms": k_avg_ms, "launches_per_step": k_n / args.steps,
@@ -300,6 +302,9 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
         "device_errors": [code, where],
     }
+
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        line["ref_gpu_kernel"] = ref_gpu_lookup(voc, desc, out, value)
 
     if not args.no_e2e:
         # end to end through the C ABI: pinned host in, pinned host out, every step.
@@ -323,17 +328,67 @@ def run_ours(args, world, rank, local):
         v, sn, dt = cpu_baseline(threads, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{sn} descriptors through a B=16 L=4 tree in {dt:.1f} s"}
-    if not args.no_scoring or args.serving:
-        del desc, out, ref32
-        torch.cuda.empty_cache()
-    if not args.no_scoring:
-        line["scoring"] = scoring_bench(args, voc, dev, world, rank)
-    if not args.no_build:
-        line["build"] = build_bench(args, dev, rank)
-    if args.serving:
-        line["serving"] = serving_bench(args, dev, rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if world > 1:
+        return  # the other workloads are single-GPU workloads
+    del desc, out, ref32
+    torch.cuda.empty_cache()
+    if not args.no_build:
+        for name, res in build_bench(args, dev, rank).items():
+            sub_line(name, res)
+    if not args.no_scoring:
+        sub_line("scoring", scoring_bench(args, voc, dev, world, rank))
+    if not args.no_serving:
+        del voc
+        torch.cuda.empty_cache()
+        sub_line("serving", serving_bench(args, dev, rank))
+
+
+def sub_line(name, res):
+    """One line per further workload after the headline, prefixed so that it does not parse as
+    the headline JSON."""
+    print(f"# {name} " + json.dumps(res), flush=True)
+
+
+def ref_gpu_build(host_desc):
+    """The reference's own GPU build (buildVocabulary: kernel_kmeansAssignCenter and
+    kernel_kmeansUpdateCenters, compiled for sm_100a from its sources into oracle/_ref) of the same
+    200,000 descriptors into a B=16, L=3 tree, capped at 10 Lloyd iterations with its own random
+    init and convergence poll every 4 iterations: median host wall time of 3 builds (the
+    descriptors are copied in inside each call, about 26 MB)."""
+    from oracle.pyoracle import Reference
+
+    if not Reference.available():
+        return {"unavailable": "reference library not built"}
+    ref = Reference()
+    ref.build_vocabulary(host_desc, 1000, 3, max_iter=10, check_interval=4)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ref.build_vocabulary(host_desc, 1000, 3, max_iter=10, check_interval=4)
+        times.append(time.perf_counter() - t0)
+    return {"value": statistics.median(times), "unit": "s", "higher_is_better": False,
+            "note": "reference init (random distinct picks), not k-means++; includes its 26 MB copy in"}
+
+
+def ref_gpu_lookup(voc, desc, ours, ours_value):
+    """The reference's own lookup kernel (kernel_VocTreeLookUp through IVocabulary::lookUp,
+    compiled for sm_100a from its sources into oracle/_ref) on the same descriptors and tree:
+    device time per launch from CUDA events, and whether its leaf IDs equal ours."""
+    import numpy as np
+
+    from oracle.pyoracle import Reference
+
+    if not Reference.available() or voc.branch_factor != 16:
+        return {"unavailable": "reference library not built or tree not 16-ary"}
+    ref = Reference()
+    host = desc.cpu().numpy()
+    got, ms = ref.lookup_device_timed(voc.serialize(), host, iters=5)
+    same = bool(np.array_equal(got, ours.cpu().numpy().view(np.uint32)))
+    n = host.shape[0]
+    return {"value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "speedup": ours_value / (n / (ms / 1e3)),
+            "kernel": "kernel_VocTreeLookUp (reference, dp4a SIMT, sm_100a)", "identical_leaf_ids": same}
 
 
 SCORING_WORKLOAD = ("inverted-file retrieval: 20,000 images of log-uniform 500-4,000 SIFT-like descriptors "
@@ -509,6 +564,7 @@ def build_bench(args, dev, rank):
                                                     np.array_equal(masks, ref["masks"]))
         out["b16_l3_200k"]["cpu_baseline"] = {"value": cpu_s, "unit": "s", "cores": 1, "kind": "port",
                                               "sample": "the same build (oracle restatement, one thread)"}
+        out["b16_l3_200k"]["ref_gpu_build"] = ref_gpu_build(host)
     del c0
     torch.cuda.empty_cache()
     c2 = sift_like(10_000_000, seed=2, n_components=4096, zipf=1.1, device=dev)
@@ -617,14 +673,9 @@ def serving_bench(args, dev, rank):
 
 
 def score_traffic(n_docs):
-    """DRAM bytes of one scoring launch from the ncu capture summarised in
-    profiles/score_kernel_20k_images.md (same seeded 20,000-image workload); None for other sizes."""
-    prof = os.path.join(ROOT, "profiles", "score_kernel_20k_images.md")
-    if n_docs != 20000 or not os.path.exists(prof):
-        return None
-    with open(prof) as fh:
-        m = re.search(r"^traffic_bytes_per_launch:\s*([0-9.]+)", fh.read(), re.M)
-    return float(m.group(1)) if m else None
+    """DRAM bytes of one scoring launch (ncu capture of the same seeded 20,000-image workload);
+    None for other sizes."""
+    return float(SCORE_DRAM_BYTES_20K_IMAGES) if n_docs == 20000 else None
 
 
 def scoring_cpu_baseline(voc, ids, doc_leaves, offs, queries, k, got_docs, got_counts, seconds):

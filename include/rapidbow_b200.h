@@ -47,7 +47,7 @@ typedef struct {
 
 /* Initial-center choice for the k-means of every node. */
 enum {
-    RBW_INIT_REFERENCE = 0, /* the reference's random distinct picks (kmeans.cpp:260-315), default seed */
+    RBW_INIT_REFERENCE = 0, /* the reference's random distinct picks (kmeans.cpp:141-196), default seed */
     RBW_INIT_KMEANSPP = 1,  /* seeded k-means++ over <= 256 sampled members per node */
     RBW_INIT_INJECTED = 2   /* caller-provided descriptor indices per node */
 };
@@ -137,7 +137,9 @@ RBW_API int rbw_voc_device_errors(const rbw_vocabulary* voc, uint32_t* code, uin
  * the GPU memory, fixed memory budgets): the same tensor-core lookup, with its working memory taken from one
  * 8 MiB device array that the library reserves on each GPU for the life of the process.
  * The first call on a device resolves that array's address and must come before any stream
- * capture; calls that may overlap on the GPU share the array and race, so serialise them.
+ * capture; the address is kept for the life of the process, so after cudaDeviceReset on that
+ * device this entry point must not be used again.  Calls that may overlap on the GPU share the
+ * array and race, so serialise them.
  * Calls needing more than 8 MiB of working memory (about one million descriptors for a
  * 16-ary, 4-level tree; see rbw_voc_lookup_scratch_bytes) fail with RBW_ERR_INVALID_ARG. */
 RBW_API int rbw_voc_lookup_noalloc(const rbw_vocabulary* voc, const void* dev_desc, uint32_t nb_desc,

@@ -33,15 +33,15 @@ def level_beg(B: int, level: int) -> int:
     return acc
 
 
-def build_oracle() -> None:
-    """Compile liborc.so (and the reference checker when its sources are present)."""
+def build_oracle(reference_dir: str | None = None) -> None:
+    """Compile liborc.so, and the reference checker when the reference sources are given
+    (``reference_dir``, else the environment variable RBW_REFERENCE_DIR) and present."""
     import subprocess
 
     subprocess.run(["make", "-C", HERE, "orc"], check=True, capture_output=True)
-    if os.path.isdir(os.environ.get("RBW_REFERENCE_DIR", "/root/reference")):
-        subprocess.run(["make", "-C", HERE, "ref",
-                        "REF=" + os.environ.get("RBW_REFERENCE_DIR", "/root/reference")],
-                       check=True, capture_output=True)
+    ref = reference_dir or os.environ.get("RBW_REFERENCE_DIR", "")
+    if ref and os.path.isdir(ref):
+        subprocess.run(["make", "-C", HERE, "ref", "REF=" + ref], check=True, capture_output=True)
 
 
 class Oracle:
@@ -211,6 +211,9 @@ class Reference:
             lib.ref_free.argtypes = [C.c_void_p]
             lib.ref_lookup.restype = C.c_int
             lib.ref_lookup.argtypes = [u8p, C.c_uint64, u8p, C.c_uint32, u32p]
+            lib.ref_lookup_device_timed.restype = C.c_int
+            lib.ref_lookup_device_timed.argtypes = [u8p, C.c_uint64, u8p, C.c_uint32, u32p, C.c_uint32,
+                                                    C.POINTER(C.c_float)]
             lib.ref_kmeans_task.restype = C.c_int
             lib.ref_kmeans_task.argtypes = [u32p, C.c_uint32, C.c_uint32, u32p, u8p, u32p, u32p, u32p, C.c_int]
             Reference._lib = lib
@@ -240,6 +243,17 @@ class Reference:
         b = np.frombuffer(blob, dtype=np.uint8).copy()
         self._check(self.lib.ref_lookup(b, b.size, desc.reshape(-1), desc.shape[0], out))
         return out
+
+    def lookup_device_timed(self, blob: bytes, desc: np.ndarray, iters: int = 5):
+        """(leaf IDs, ms per launch) of the reference lookup kernel on descriptors already in
+        device memory (launches bracketed by CUDA events; the copy in is not timed)."""
+        desc = np.ascontiguousarray(desc, dtype=np.uint8)
+        out = np.empty(desc.shape[0], dtype=np.uint32)
+        b = np.frombuffer(blob, dtype=np.uint8).copy()
+        ms = C.c_float()
+        self._check(self.lib.ref_lookup_device_timed(b, b.size, desc.reshape(-1), desc.shape[0], out, iters,
+                                                     C.byref(ms)))
+        return out, float(ms.value)
 
     def kmeans_task(self, tiles_words, nb_desc, centers_words, assign, do_update):
         tiles_words = np.ascontiguousarray(tiles_words, dtype=np.uint32)

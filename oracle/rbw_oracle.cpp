@@ -121,7 +121,7 @@ void assignNode(const uint8_t* desc, const uint32_t* members, uint32_t n, const 
     }
 }
 
-// randPick (kmeans.cpp:260-287): min(n, nbToPick) distinct random members, sorted, padded with
+// randPick (kmeans.cpp:141-168): min(n, nbToPick) distinct random members, sorted, padded with
 // the last pick.  `rng` is the caller's state (the reference keeps one thread_local engine).
 uint32_t randPick(std::mt19937_64& rng, uint32_t* dst, uint32_t randSpace, uint32_t nbToPick)
 {
@@ -189,7 +189,7 @@ void orc_kmeans_update(const uint32_t* counts, const uint64_t* sums, uint32_t B,
 uint32_t orc_kmeanspp_init(const uint8_t* desc, const uint32_t* members, uint32_t n, uint32_t B, uint64_t seed,
                            uint32_t level, uint64_t nodeInLevel, uint32_t* pickedDesc)
 {
-    // Seeded k-means++ over at most 256 sampled members (the scheme kmeans.cpp:301-302 sketches).
+    // Seeded k-means++ over at most 256 sampled members (the scheme kmeans.cpp:182-183 sketches).
     uint64_t s = seed ^ (uint64_t(level) * 0x9E3779B97F4A7C15ull) ^ (nodeInLevel * 0xD1B54A32D192ED03ull);
     if (n == 0) {
         for (uint32_t b = 0; b < B; b++) pickedDesc[b] = kInvalid;
@@ -252,7 +252,7 @@ int orc_build_vocabulary(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, u
     const uint64_t nbNodes = levelBeg(B, L);
     std::fill(masks, masks + nbNodes, 0u);
     std::fill(occ, occ + nbNodes * B, 0u);
-    std::mt19937_64 rng{}; // kmeans.cpp:264, a fresh thread's engine
+    std::mt19937_64 rng{}; // kmeans.cpp:145, a fresh thread's engine
     // Groups of the current level, in breadth-first order (Vocabulary.cpp:50-52).
     std::vector<std::vector<uint32_t>> groups{std::vector<uint32_t>(nbDesc)};
     std::iota(groups[0].begin(), groups[0].end(), 0u);
@@ -268,13 +268,13 @@ int orc_build_vocabulary(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, u
             std::vector<uint32_t> picks(B, kInvalid);
             uint32_t nValid = 0;
             if (initMode == ORC_INIT_REFERENCE) {
-                // makeRandCenters (kmeans.cpp:289-315) + launchKMeansInitCenters (reformatDesc.cu:88-96)
+                // makeRandCenters (kmeans.cpp:170-196) + launchKMeansInitCenters (reformatDesc.cu:88-96)
                 std::vector<uint32_t> tmp(B);
                 nValid = randPick(rng, tmp.data(), n, B);
                 if (n != 0) {
                     for (uint32_t b = 0; b < B; b++) picks[b] = members[tmp[b]];
                 } else {
-                    // An empty group reads grpIndices[0] at its padded offset (kmeans.cpp:298-305):
+                    // An empty group reads grpIndices[0] at its padded offset (kmeans.cpp:179-186):
                     // the first member of the next non-empty group of this level, if any.
                     uint32_t v = kInvalid;
                     for (uint64_t h = g + 1; h < nbGroups; h++) {
@@ -301,7 +301,7 @@ int orc_build_vocabulary(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, u
                 }
             }
             masks[lb + g] = nValid >= 32 ? 0xFFFFFFFFu : ((1u << nValid) - 1u);
-            // ---- Lloyd iterations (kmeans.cpp:237-252 with kmeans.cu:238-240,341-343):
+            // ---- Lloyd iterations (kmeans.cpp:118-133 with kmeans.cu:238-240,341-343):
             // a node whose last iteration changed nothing is frozen; the convergence-check
             // interval only decides when the host stops and does not change any node's result.
             std::vector<uint8_t> assign(n, 0); // fresh (zeroed) assignment memory
@@ -328,7 +328,7 @@ int orc_build_vocabulary(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, u
         }
         groups.swap(next);
     }
-    // idf-like weights (Vocabulary.cpp:202-207)
+    // idf-like weights (Vocabulary.cpp:103-108)
     for (uint64_t i = 0; i < nbNodes * B; i++) {
         weights[i] = occ[i] == 0 ? std::numeric_limits<float>::min()
                                  : std::max(std::numeric_limits<float>::min(),

@@ -3,7 +3,7 @@
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs may load this library,
  * and only as the checker / the timed CPU baseline -- never as the product path.
  *
- * Layouts (shared with the product, documented in DESIGN.md):
+ * Layouts (shared with the product):
  *   descriptors : uint8 [n][128], row-major.
  *   centers     : uint8 [levelBeg(L)][B][128]; node index = breadth-first (levelBeg(l) + i).
  *                 For B = 16 this is the reference's Node (uint32[32 words][16 centers],
@@ -40,15 +40,19 @@ void orc_kmeans_update(const uint32_t* counts, const uint64_t* sums, uint32_t B,
 
 enum { ORC_INIT_REFERENCE = 0, ORC_INIT_KMEANSPP = 1, ORC_INIT_INJECTED = 2 };
 
-/* Initial centers of one node for ORC_INIT_KMEANSPP (seeded k-means++ over <= 256 sampled
- * members; the spec is in DESIGN.md).  Returns the number of distinct picks. */
+/* Initial centers of one node for ORC_INIT_KMEANSPP: seeded k-means++ over <= 256 sampled members.
+ * SplitMix64 stream seeded with seed ^ level * 0x9E3779B97F4A7C15 ^ node * 0xD1B54A32D192ED03; Floyd
+ * sampling of min(n, 256) member positions (sorted); the first center uniform over the sample;
+ * then D^2 sampling with exact integer squared distances (smallest i with prefix > draw % total);
+ * stops early when every sampled member coincides with a chosen center.  Padding repeats the last
+ * pick.  Returns the number of distinct picks. */
 uint32_t orc_kmeanspp_init(const uint8_t* desc, const uint32_t* members, uint32_t n, uint32_t B,
                            uint64_t seed, uint32_t level, uint64_t nodeInLevel, uint32_t* pickedDesc);
 
-/* Hierarchical k-means vocabulary build (Vocabulary.cpp:32-121, kmeans.cpp:27-343).
+/* Hierarchical k-means vocabulary build (Vocabulary.cpp:32-121, kmeans.cpp:27-225).
  *   maxIter : Lloyd cap (reference default 1000);
  *   initMode: ORC_INIT_REFERENCE (randPick with a fresh default-seeded mt19937_64,
- *             kmeans.cpp:260-315), ORC_INIT_KMEANSPP (seeded), ORC_INIT_INJECTED (injected[],
+ *             kmeans.cpp:141-196), ORC_INIT_KMEANSPP (seeded), ORC_INIT_INJECTED (injected[],
  *             B descriptor indices per node in breadth-first order; UINT32_MAX = invalid).
  *   outputs : centers, masks, weights as documented above; occ [levelBeg(L)][B];
  *             itersOut [levelBeg(L)] = Lloyd iterations each node ran (may be NULL).

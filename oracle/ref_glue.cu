@@ -144,7 +144,7 @@ int ref_db_query_batch(const void* db, const uint32_t* leaves, const uint64_t* o
 
 // ---------------------------------------------------------------- GPU: vocabulary
 // Builds a vocabulary with the reference (fresh thread, so its thread_local init RNG starts
-// from the default seed, kmeans.cpp:264) and returns the serialized blob
+// from the default seed, kmeans.cpp:145) and returns the serialized blob
 // (Vocabulary.cpp:175-198).  maxIter == 0 keeps the reference defaults (1000 iterations,
 // check interval 4); otherwise the level loop of Vocabulary.cpp:66-99 is re-driven with a
 // KMeans whose cap and check interval are set.

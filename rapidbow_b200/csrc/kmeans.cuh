@@ -45,7 +45,7 @@ void buildNodeTiles(const uint32_t* nodeCnt, const uint32_t* nodeOff, uint32_t n
                     cudaStream_t s);
 
 // Initial centers: centers[g][b] = desc[members[nodeOff[g] + pos[g][b]]], or 0xFF bytes when the
-// position is past the member array / invalid (reformatDesc.cu:88-96 with kmeans.cpp:298-305).
+// position is past the member array / invalid (reformatDesc.cu:88-96 with kmeans.cpp:179-186).
 void launchInitCenters(const KMeansLevel& lv, const uint32_t* pos, uint64_t nbDescTotal, cudaStream_t s);
 // Initial centers from descriptor indices (kInvalidIdx -> 0xFF bytes): injected initialisation.
 void launchInitCentersFromDesc(const KMeansLevel& lv, const uint32_t* descIdx, uint64_t nbDescTotal, cudaStream_t s);

@@ -3,14 +3,15 @@
 //
 // Two implementations behind launchLookup():
 //   * lookupPassTc  : tcgen05 kind::i8 (u8 x u8 -> s32, exact) over level pairs.  A pass takes
-//                     the descriptors grouped by their node at level 2p, stages 128-row tiles with
-//                     TMA (tiled load for the first pass, tile::gather4 through a permutation
-//                     afterwards), runs one MMA against the node's 16 centers (level 2p) and one
-//                     against all of its children's centers (level 2p+1, N = 16*B), and picks the
-//                     argmin of |c|^2 - 2 x.c from tensor memory.  Between passes a device
+//                     the descriptors grouped by their node at level 2p, stages 128-row tiles in
+//                     shared memory (a TMA tiled load in input order for the first pass, a 16-byte
+//                     cp.async gather through the permutation afterwards), runs one MMA against
+//                     the node's 16 centers (level 2p) and one against all of its children's
+//                     centers (level 2p+1, N = 16*B), and picks the argmin of |c|^2 - 2 x.c
+//                     from tensor memory.  Between passes a device
 //                     counting sort (histogram fused into the pass epilogue, scan, scatter)
 //                     groups the descriptors by their node at level 2p+2.
-//   * lookupSimtF32 : plain FP32 SIMT kernel (16 threads per descriptor, one center each),
+//   * lookupSimtF32 : plain FP32 SIMT kernel (one thread per descriptor, 16 fp32 accumulators),
 //                     the comparison baseline.  Exact for uint8 data (all sums < 2^24).
 #include "lookup.cuh"
 #include "timing.h"
@@ -638,7 +639,15 @@ __global__ void __launch_bounds__(kScatterThreads) scatterRows(const uint32_t* n
 }
 
 // ------------------------------------------------------------------ plain FP32 SIMT kernel
-constexpr uint32_t kSimtDesc = 16; // descriptors per CTA, 16 threads each
+// One thread per descriptor.  The block's 128 descriptor rows are staged once in shared memory
+// (coalesced 16-byte loads; rows padded to 144 bytes so that the eight 16-byte reads of a
+// quarter warp fall in distinct banks).  Per level the thread walks its row in 16-dimension
+// chunks: the chunk is converted to fp32 once and multiplied into 16 fp32 accumulators, one per
+// center, whose bytes are read as 16-byte vectors from the tree (L1/L2) and converted to fp32
+// on the fly.  Every partial sum is an integer below 2^24, so the fp32 dot products -- and
+// |c|^2 - 2 x.c -- are exact and the argmin (lowest index on ties) equals the reference's.
+constexpr uint32_t kSimtThreads = 128;
+constexpr uint32_t kSimtRowStride = kDims + 16;
 
 __device__ __forceinline__ float byteToFloat(uint32_t word, uint32_t k)
 {
@@ -646,54 +655,68 @@ __device__ __forceinline__ float byteToFloat(uint32_t word, uint32_t k)
     return __int_as_float(static_cast<int>(__byte_perm(word, 0x4B000000u, 0x7540u | k))) - 8388608.0f;
 }
 
-__global__ void __launch_bounds__(256) lookupSimtF32(const uint8_t* __restrict__ centers,
-                                                     const int32_t* __restrict__ cnorm, uint32_t B, uint32_t L,
-                                                     const uint8_t* __restrict__ desc, uint64_t n,
-                                                     uint32_t* __restrict__ out)
+__global__ void __launch_bounds__(kSimtThreads, 8) lookupSimtF32(const uint8_t* __restrict__ centers,
+                                                              const int32_t* __restrict__ cnorm, uint32_t B,
+                                                              uint32_t L, const uint8_t* __restrict__ desc,
+                                                              uint64_t n, uint32_t* __restrict__ out)
 {
-    __shared__ float xs[kSimtDesc][kDims + 4];
-    const uint32_t g = threadIdx.x / 16, j = threadIdx.x % 16;
-    const uint64_t descBase = uint64_t(blockIdx.x) * kSimtDesc;
-    if (threadIdx.x < kSimtDesc * 8) {
-        const uint32_t d = threadIdx.x / 8, part = threadIdx.x % 8;
+    __shared__ __align__(16) uint8_t xs[kSimtThreads * kSimtRowStride];
+    const uint64_t base = uint64_t(blockIdx.x) * kSimtThreads;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; k++) {
+        const uint32_t i = k * kSimtThreads + threadIdx.x; // 16-byte chunk i % 8 of row i / 8
+        const uint32_t r = i / 8, c = i % 8;
         uint4 v = make_uint4(0, 0, 0, 0);
-        if (descBase + d < n) v = __ldg(reinterpret_cast<const uint4*>(desc + (descBase + d) * kDims) + part);
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (uint32_t q = 0; q < 4; q++)
-#pragma unroll
-            for (uint32_t k = 0; k < 4; k++) xs[d][part * 16 + q * 4 + k] = byteToFloat(w[q], k);
+        if (base + r < n) v = __ldg(reinterpret_cast<const uint4*>(desc + (base + r) * kDims) + c);
+        *reinterpret_cast<uint4*>(xs + r * kSimtRowStride + c * 16) = v;
     }
     __syncthreads();
+    const uint8_t* x = xs + threadIdx.x * kSimtRowStride;
     uint64_t idx = 0, lb = 0;
     for (uint32_t level = 0; level < L; level++) {
         const uint64_t node = lb + idx;
-        const uint4* c = reinterpret_cast<const uint4*>(centers + (node * kMaxBranch + j) * kDims);
-        float acc = 0.f;
+        const uint4* c4 = reinterpret_cast<const uint4*>(centers + node * kMaxBranch * kDims);
+        float acc[kMaxBranch];
 #pragma unroll
-        for (uint32_t part = 0; part < 8; part++) {
-            const uint4 v = __ldg(c + part);
-            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        for (uint32_t b = 0; b < kMaxBranch; b++) acc[b] = 0.f;
+#pragma unroll 1
+        for (uint32_t chunk = 0; chunk < 8; chunk++) {
+            const uint4 xv = *reinterpret_cast<const uint4*>(x + chunk * 16);
+            const uint32_t xw[4] = {xv.x, xv.y, xv.z, xv.w};
+            float xf[16];
 #pragma unroll
             for (uint32_t q = 0; q < 4; q++)
 #pragma unroll
-                for (uint32_t k = 0; k < 4; k++) acc = fmaf(xs[g][part * 16 + q * 4 + k], byteToFloat(w[q], k), acc);
-        }
-        float s = j < B ? static_cast<float>(__ldg(cnorm + node * kMaxBranch + j)) - 2.f * acc : INFINITY;
-        uint32_t bj = j;
+                for (uint32_t k = 0; k < 4; k++) xf[4 * q + k] = byteToFloat(xw[q], k);
 #pragma unroll
-        for (uint32_t off = 8; off > 0; off >>= 1) {
-            const float os = __shfl_xor_sync(0xFFFFFFFFu, s, off, 16);
-            const uint32_t oj = __shfl_xor_sync(0xFFFFFFFFu, bj, off, 16);
-            if (os < s || (os == s && oj < bj)) {
-                s = os;
-                bj = oj;
+            for (uint32_t b = 0; b < kMaxBranch; b++) {
+                if (b < B) {
+                    const uint4 cv = __ldg(c4 + b * 8 + chunk);
+                    const uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
+#pragma unroll
+                    for (uint32_t q = 0; q < 4; q++)
+#pragma unroll
+                        for (uint32_t k = 0; k < 4; k++) acc[b] = fmaf(xf[4 * q + k], byteToFloat(cw[q], k), acc[b]);
+                }
             }
         }
-        idx = idx * B + bj;
+        const int32_t* cn = cnorm + node * kMaxBranch;
+        float best = static_cast<float>(__ldg(cn)) - 2.f * acc[0];
+        uint32_t bi = 0;
+#pragma unroll
+        for (uint32_t b = 1; b < kMaxBranch; b++) {
+            if (b < B) {
+                const float s = static_cast<float>(__ldg(cn + b)) - 2.f * acc[b];
+                if (s < best) {
+                    best = s;
+                    bi = b;
+                }
+            }
+        }
+        idx = idx * B + bi;
         lb = lb * B + 1;
     }
-    if (j == 0 && descBase + g < n) out[descBase + g] = static_cast<uint32_t>(idx);
+    if (base + threadIdx.x < n) out[base + threadIdx.x] = static_cast<uint32_t>(idx);
 }
 
 // ------------------------------------------------------------------ host side
@@ -729,18 +752,6 @@ CUtensorMap makeRowMap(const uint8_t* desc, uint64_t n, uint32_t boxRows)
                                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw Error(kCudaError, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
     return m;
-}
-
-int smCount()
-{
-    static int sms = 0;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        int dev = 0;
-        RBW_CUDA(cudaGetDevice(&dev));
-        RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    });
-    return sms;
 }
 
 uint32_t maxBinsFor(uint32_t B, uint32_t L)
@@ -786,22 +797,20 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
 {
     if (n == 0) return 0;
     if (algo == kLookupSimtF32) {
-        const uint64_t blocks = (n + kSimtDesc - 1) / kSimtDesc;
+        const uint64_t blocks = (n + kSimtThreads - 1) / kSimtThreads;
         ScopedKernelTimer timer(kTimedLookupSimt, stream);
-        lookupSimtF32<<<static_cast<uint32_t>(blocks), 256, 0, stream>>>(tree.centers, tree.cnorm, tree.B, tree.L, desc,
+        lookupSimtF32<<<static_cast<uint32_t>(blocks), kSimtThreads, 0, stream>>>(tree.centers, tree.cnorm, tree.B, tree.L, desc,
                                                                          n, leaf);
         RBW_CUDA(cudaGetLastError());
         return 1;
     }
-    static std::once_flag attrOnce;
-    std::call_once(attrOnce, [] {
-        RBW_CUDA(cudaFuncSetAttribute(lookupPassTc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(kTcSmemBytes)));
-    });
+    static std::atomic<uint64_t> attrSet{0};
+    setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(lookupPassTc), static_cast<int>(kTcSmemBytes),
+                                   attrSet);
     const CUtensorMap tmapTile = makeRowMap(desc, n, kTileRows);
     const uint32_t B = tree.B, L = tree.L;
     const uint32_t passes = (L + 1) / 2;
-    const uint32_t grid = static_cast<uint32_t>(smCount());
+    const uint32_t grid = static_cast<uint32_t>(currentSmCount());
     const uint64_t bins = L > 2 ? maxBinsFor(B, L) : 0;
     uint32_t* count = scratch.bins;
     uint32_t* rowOff = count ? count + bins : nullptr;

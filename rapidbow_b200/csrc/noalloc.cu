@@ -11,7 +11,10 @@
 //
 // Rules for callers:
 //   * the first call on a device looks the array's device address up (cudaGetSymbolAddress)
-//     with that device current; make that first call before any stream capture begins;
+//     with that device current; make that first call before any stream capture begins.  The
+//     address is kept for the life of the process: after cudaDeviceReset on that device the
+//     module is loaded again and the kept address is stale, so the entry point must not be used
+//     after a device reset;
 //   * all calls on a device share the one array: calls whose kernels may overlap on the GPU
 //     (different streams without ordering between them, or several host threads) race on it
 //     and must be serialised by the caller;
@@ -36,10 +39,8 @@ static __device__ __align__(256) unsigned char gNoAllocScratch[kNoAllocScratchBy
 void* noAllocScratchAddress()
 {
     static std::mutex mu;
-    static void* addr[64] = {};
-    int dev = 0;
-    RBW_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) throw Error(kUnsupported, "device ordinal out of range");
+    static void* addr[kMaxDevices] = {};
+    const int dev = currentDevice();
     std::lock_guard<std::mutex> lk(mu);
     if (addr[dev] == nullptr) {
         void* p = nullptr;

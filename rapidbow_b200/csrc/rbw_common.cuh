@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -58,6 +59,43 @@ inline uint64_t ipow(uint64_t b, uint32_t e)
 }
 template <typename T>
 __host__ __device__ constexpr T ceilDiv(T a, T b) { return (a + b - 1) / b; }
+
+constexpr int kMaxDevices = 64;
+
+// Ordinal of the calling thread's current device.  Per-device state (function attributes, SM
+// counts, pools) is keyed by it: attributes such as the dynamic shared-memory limit belong to
+// one device's context and must be set again for every other device the process uses.
+inline int currentDevice()
+{
+    int dev = 0;
+    RBW_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw Error(kUnsupported, "device ordinal out of range");
+    return dev;
+}
+
+// Number of SMs of the current device.
+inline int currentSmCount()
+{
+    static std::atomic<int> sms[kMaxDevices] = {};
+    const int dev = currentDevice();
+    int v = sms[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        RBW_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        sms[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+// Sets a kernel's dynamic shared-memory limit once per device (idempotent, so a race between
+// two threads only sets it twice).
+inline void setMaxDynamicSmemOncePerDevice(const void* kernel, int bytes, std::atomic<uint64_t>& doneMask)
+{
+    const int dev = currentDevice();
+    const uint64_t bit = uint64_t(1) << dev;
+    if (doneMask.load(std::memory_order_acquire) & bit) return;
+    RBW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    doneMask.fetch_or(bit, std::memory_order_acq_rel);
+}
 
 // Device-side error record written by bounded waits and bounds checks.
 struct DeviceErrors {

@@ -1,5 +1,5 @@
 // Vocabulary: tree storage, GPU hierarchical k-means build, lookup dispatch and the blob format.
-//   build        : Vocabulary.cpp:32-121 + kmeans.cpp:27-343, all nodes of a level per launch
+//   build        : Vocabulary.cpp:32-121 + kmeans.cpp:27-225, all nodes of a level per launch
 //   lookup       : Vocabulary.h:59-63 / Vocabulary.cpp:162-173
 //   serialize    : Vocabulary.cpp:175-198 (byte-compatible for B = 16)
 //   deserialize  : Vocabulary.cpp:126-157
@@ -95,7 +95,7 @@ __global__ void iotaKernel(uint32_t* p, uint64_t n)
 
 uint32_t blocksFor(uint64_t n, uint32_t t) { return static_cast<uint32_t>((n + t - 1) / t); }
 
-// The reference's initial pick (kmeans.cpp:260-287): min(n, k) distinct members drawn from one
+// The reference's initial pick (kmeans.cpp:141-168): min(n, k) distinct members drawn from one
 // default-seeded std::mt19937_64 that lives for the whole build (a fresh thread's
 // thread_local engine), sorted and padded with the last pick.  The steps -- `rng() % n` into a
 // hash set when n > 16*k, std::shuffle of 0..n-1 otherwise -- have to be the same calls on the
@@ -120,7 +120,7 @@ uint32_t referencePick(std::mt19937_64& rng, uint32_t* dst, uint32_t space, uint
 
 float idfWeight(uint32_t nbDoc, uint32_t occ)
 {
-    // Vocabulary.cpp:202-207
+    // Vocabulary.cpp:103-108
     return occ == 0 ? std::numeric_limits<float>::min()
                     : std::max(std::numeric_limits<float>::min(), std::log(float(nbDoc) / float(occ)));
 }
@@ -384,7 +384,7 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
 
     std::vector<uint32_t> occ(voc->mNbNodes * B, 0u);
     voc->mMasks.assign(voc->mNbNodes, 0u);
-    std::mt19937_64 rng{}; // kmeans.cpp:264 (default seed)
+    std::mt19937_64 rng{}; // kmeans.cpp:145 (default seed)
     std::vector<uint32_t> hostCnt, hostPicks, hostNValid;
     if (stats) *stats = BuildStats{};
 
@@ -450,7 +450,7 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
         }
         launchCenterNorms(lv, stream);
 
-        // ---- Lloyd iterations (kmeans.cpp:237-252)
+        // ---- Lloyd iterations (kmeans.cpp:118-133)
         buildNodeTiles(lv.nodeCnt, lv.nodeOff, nbLv, 128, tileOff.as<uint32_t>(), scanTmp.as<uint32_t>(),
                        tiles128.as<NodeTile>(), maxTiles128, totals, stream);
         RBW_CUDA(cudaMemsetAsync(assign.get(), 0, n, stream)); // fresh (zeroed) assignment memory
