@@ -53,8 +53,28 @@ enum {
 };
 
 /* Build flags.  The reference rounds centers with its --use_fast_math division
- * (kmeans.cu:367); RBW_BUILD_IEEE_DIVISION uses the correctly rounded quotient instead. */
-enum { RBW_BUILD_IEEE_DIVISION = 1 };
+ * (kmeans.cu:367); RBW_BUILD_IEEE_DIVISION uses the correctly rounded quotient instead.
+ * RBW_BUILD_FLOAT_CENTERS (no counterpart in the reference, whose centers are uint8) keeps fp32
+ * centers, c = float(double(sum) / double(count)) of the exact integer sums; distances come from
+ * the tensor cores with each center split into hi + lo bf16 parts and fp32 accumulation, and
+ * every descriptor whose best-versus-second margin is within the stated error bound is re-scored
+ * in FP64 on the GPU, so assignments equal those of an FP64 evaluation (lowest index on ties).
+ * Lookups through such a vocabulary use the same arithmetic. */
+enum { RBW_BUILD_IEEE_DIVISION = 1, RBW_BUILD_FLOAT_CENTERS = 2 };
+
+/* Center storage of a vocabulary. */
+enum { RBW_CENTERS_UINT8 = 0, RBW_CENTERS_FLOAT32 = 1 };
+
+/* Statistics of the build that made a vocabulary (zero for uploaded or deserialised ones). */
+typedef struct {
+    uint32_t levels;
+    uint32_t iterations[16];     /* Lloyd steps run per level */
+    double inertia_first[16];    /* float centers: FP64 inertia of the level's first assignment */
+    double inertia_last[16];     /*                and of its last one (frozen nodes keep theirs) */
+    uint64_t refined[16];        /* float centers: assignments re-scored in FP64, all steps */
+    uint64_t assignments[16];    /*                assignments made, all steps */
+    double seconds;              /* wall time of the build call */
+} rbw_build_stats;
 
 typedef struct {
     uint32_t max_iterations;       /* Lloyd cap; reference: 1000 (kmeans.h:118) */
@@ -89,6 +109,11 @@ RBW_API int rbw_voc_build(rbw_desc_attr attr, uint32_t branch_factor, const void
  * [levelBeg(L)], weights [levelBeg(L)][B] (the fields of Vocabulary, Vocabulary.h:44-51). */
 RBW_API int rbw_voc_from_host(uint32_t branch_factor, uint32_t nb_levels, const uint8_t* centers,
                               const uint32_t* masks, const float* weights, rbw_vocabulary** out);
+
+/* rbw_voc_from_host with fp32 centers [levelBeg(L)][B][128] (no counterpart in the reference):
+ * a float-center vocabulary (see RBW_BUILD_FLOAT_CENTERS). */
+RBW_API int rbw_voc_from_host_f32(uint32_t branch_factor, uint32_t nb_levels, const float* centers,
+                                  const uint32_t* masks, const float* weights, rbw_vocabulary** out);
 
 /* Replaces IVocabulary::lookUp (RapidBoW.h:66-68, Vocabulary.h:59-63): leaf index per descriptor
  * in [0, B^L), asynchronous on `stream`, device buffers. */
@@ -125,6 +150,20 @@ RBW_API int rbw_voc_level_weights(const rbw_vocabulary* voc, uint32_t level, con
 RBW_API int rbw_voc_get_tree(const rbw_vocabulary* voc, uint8_t* host_centers, uint32_t* host_masks,
                              float* host_weights);
 
+/* No counterpart in the reference.  *type = RBW_CENTERS_UINT8 or RBW_CENTERS_FLOAT32. */
+RBW_API int rbw_voc_center_type(const rbw_vocabulary* voc, int32_t* type);
+
+/* fp32 centers [levelBeg(L)][B][128] of a float-center vocabulary (RBW_ERR_UNSUPPORTED for a
+ * uint8 one, whose centers rbw_voc_get_tree returns; for a float one that returns them rounded). */
+RBW_API int rbw_voc_get_centers_f32(const rbw_vocabulary* voc, float* host_centers);
+
+/* Statistics of the build that made the vocabulary (no counterpart in the reference). */
+RBW_API int rbw_voc_build_stats(const rbw_vocabulary* voc, rbw_build_stats* stats);
+
+/* Reads and clears how many lookup descriptors were re-scored in FP64 since the last call
+ * (float-center vocabularies; 0 otherwise).  Synchronizes the device. */
+RBW_API int rbw_voc_refined_lookups(const rbw_vocabulary* voc, uint64_t* refined);
+
 /* Device scratch bytes rbw_voc_lookup needs for nb_desc descriptors. */
 RBW_API int rbw_voc_lookup_scratch_bytes(const rbw_vocabulary* voc, uint64_t nb_desc, uint64_t* bytes);
 
@@ -141,7 +180,8 @@ RBW_API int rbw_voc_device_errors(const rbw_vocabulary* voc, uint32_t* code, uin
  * device this entry point must not be used again.  Calls that may overlap on the GPU share the
  * array and race, so serialise them.
  * Calls needing more than 8 MiB of working memory (about one million descriptors for a
- * 16-ary, 4-level tree; see rbw_voc_lookup_scratch_bytes) fail with RBW_ERR_INVALID_ARG. */
+ * 16-ary, 4-level tree; see rbw_voc_lookup_scratch_bytes) fail with RBW_ERR_INVALID_ARG, and
+ * float-center vocabularies with RBW_ERR_UNSUPPORTED. */
 RBW_API int rbw_voc_lookup_noalloc(const rbw_vocabulary* voc, const void* dev_desc, uint32_t nb_desc,
                                    uint32_t* dev_leaf, void* stream);
 
@@ -154,7 +194,8 @@ RBW_API void rbw_voc_destroy(rbw_vocabulary* voc);
  * distances.  The index lives on the GPU.  Adds are staged on the host and indexed on the
  * device at the next query, in work proportional to the documents added (a delta segment,
  * merged into the main segment from time to time), ordered with queries by CUDA events.
- * Documents and queries hold at most 32768 descriptors; max_results at most 1024.
+ * Documents, queries and max_results have no size limit beyond memory (items above 32768
+ * descriptors are sorted in global memory, result sets above 1024 selected there).
  * Results are ordered by ascending score, ties by ascending document id (the reference's
  * std::sort leaves the order of equal scores unspecified). */
 typedef struct rbw_database rbw_database;
@@ -219,9 +260,11 @@ RBW_API int rbw_db_postings(const rbw_database* db, uint32_t leaf, uint32_t* out
  * database one image at a time.  A server answers query images (host descriptors) with their
  * top-k documents (lookup + scoring) and batches them continuously: a batch is formed from the
  * waiting requests, in arrival order, as soon as one of max_inflight_batches slots is free and
- * only while its device-memory estimate fits what the batches in flight leave of
- * hbm_budget_bytes; each batch runs on its own stream, so batches overlap on the GPU and
- * requests that arrive meanwhile join the next one.  Results do not depend on the batching. */
+ * only while its device-memory estimate fits both what the batches in flight leave of
+ * hbm_budget_bytes and the device memory free at that moment (the driver's free memory plus
+ * what the library's pool holds unused, less 256 MiB; this check is skipped while no batch is
+ * in flight); each batch runs on its own stream, so batches overlap on the GPU and requests
+ * that arrive meanwhile join the next one.  Results do not depend on the batching. */
 typedef struct rbw_server rbw_server;
 
 typedef struct {
@@ -229,7 +272,7 @@ typedef struct {
     uint32_t max_inflight_batches;  /* batches on the GPU at once (default 3) */
     uint64_t max_batch_descriptors; /* descriptors per batch (default 2^21) */
     uint64_t hbm_budget_bytes;      /* device memory for batches; 0 = half the free memory at creation */
-    uint32_t max_results;           /* k of every request, 1..1024 (default 100) */
+    uint32_t max_results;           /* k of every request, >= 1 (default 100) */
 } rbw_server_options;
 
 typedef struct {

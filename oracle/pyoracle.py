@@ -67,6 +67,14 @@ class Oracle:
             lib.orc_build_vocabulary.argtypes = [u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                                  C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
                                                  u8p, u32p, f32p, u32p, u32p]
+            lib.orc_dist64.restype = C.c_double
+            lib.orc_dist64.argtypes = [u8p, f32p]
+            lib.orc_lookup_f32.restype = None
+            lib.orc_lookup_f32.argtypes = [f32p, C.c_uint32, C.c_uint32, u8p, C.c_uint64, u32p, C.c_uint32]
+            lib.orc_build_vocabulary_f32.restype = C.c_int
+            lib.orc_build_vocabulary_f32.argtypes = [u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                                     C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p,
+                                                     f32p, u32p, f32p, u32p, u32p, f64p, f64p, C.c_uint32]
             lib.orc_db_create.restype = C.c_void_p
             lib.orc_db_create.argtypes = [C.c_uint32, C.c_uint32, f32p]
             lib.orc_db_destroy.restype = None
@@ -136,6 +144,41 @@ class Oracle:
         if rc != 0:
             raise ValueError("oracle build rejected its input")
         return dict(centers=centers, masks=masks, weights=weights, occ=occ, iters=iters)
+
+    # ---------------------------------------------------------------- float-center mode
+    def dist64(self, x: np.ndarray, c: np.ndarray) -> float:
+        return float(self.lib.orc_dist64(np.ascontiguousarray(x, dtype=np.uint8),
+                                         np.ascontiguousarray(c, dtype=np.float32)))
+
+    def lookup_f32(self, centers: np.ndarray, B: int, L: int, desc: np.ndarray, threads: int = 1) -> np.ndarray:
+        desc = np.ascontiguousarray(desc, dtype=np.uint8)
+        out = np.empty(desc.shape[0], dtype=np.uint32)
+        self.lib.orc_lookup_f32(np.ascontiguousarray(centers, dtype=np.float32).reshape(-1), B, L,
+                                desc.reshape(-1), desc.shape[0], out, threads)
+        return out
+
+    def build_vocabulary_f32(self, desc, nb_doc, B, L, max_iter=1000, init=INIT_REFERENCE, seed=0, injected=None,
+                             threads: int = 1):
+        desc = np.ascontiguousarray(desc, dtype=np.uint8)
+        nodes = level_beg(B, L)
+        centers = np.empty((nodes, B, 128), dtype=np.float32)
+        masks = np.empty(nodes, dtype=np.uint32)
+        weights = np.empty((nodes, B), dtype=np.float32)
+        occ = np.empty((nodes, B), dtype=np.uint32)
+        iters = np.empty(nodes, dtype=np.uint32)
+        first = np.empty(L, dtype=np.float64)
+        last = np.empty(L, dtype=np.float64)
+        inj = None
+        if injected is not None:
+            injected = np.ascontiguousarray(injected, dtype=np.uint32)
+            inj = injected.ctypes.data_as(C.c_void_p)
+        rc = self.lib.orc_build_vocabulary_f32(desc.reshape(-1), desc.shape[0], nb_doc, B, L, max_iter, init, seed,
+                                               inj, centers.reshape(-1), masks, weights.reshape(-1),
+                                               occ.reshape(-1), iters, first, last, threads)
+        if rc != 0:
+            raise ValueError("oracle build rejected its input")
+        return dict(centers=centers, masks=masks, weights=weights, occ=occ, iters=iters, inertia_first=first,
+                    inertia_last=last)
 
     # ---------------------------------------------------------------- DataBase
     def db(self, B: int, L: int, weights: np.ndarray) -> "OracleDb":

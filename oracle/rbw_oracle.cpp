@@ -6,6 +6,7 @@
 #include "rbw_oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -329,6 +330,289 @@ int orc_build_vocabulary(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, u
         groups.swap(next);
     }
     // idf-like weights (Vocabulary.cpp:103-108)
+    for (uint64_t i = 0; i < nbNodes * B; i++) {
+        weights[i] = occ[i] == 0 ? std::numeric_limits<float>::min()
+                                 : std::max(std::numeric_limits<float>::min(),
+                                            std::log(float(nbDoc) / float(occ[i])));
+    }
+    return 0;
+}
+
+} // extern "C"
+
+// ------------------------------------------------------------------ float-center mode
+namespace {
+
+// orc_dist64's evaluation order: 32 lane partials of four fused multiply-adds, then a butterfly
+// of pairwise sums (each level adds the partner that differs in one index bit; the sums are
+// symmetric, so lane l < off keeps p_l + p_(l+off)).  Operands come "lane-major transposed":
+// v[32 k + l] holds element 4 l + k, so every step is a contiguous vector operation.
+static inline __attribute__((always_inline)) double dist64T(const double* __restrict__ xT,
+                                                           const double* __restrict__ cT)
+{
+    double p[32];
+    for (uint32_t l = 0; l < 32; l++) p[l] = 0.0;
+    for (uint32_t k = 0; k < 4; k++) {
+        for (uint32_t l = 0; l < 32; l++) {
+            const double e = xT[32 * k + l] - cT[32 * k + l];
+            p[l] = std::fma(e, e, p[l]);
+        }
+    }
+    for (uint32_t off = 16; off > 0; off >>= 1)
+        for (uint32_t l = 0; l < off; l++) p[l] = p[l] + p[l + off];
+    return p[0];
+}
+
+template <typename T>
+static inline __attribute__((always_inline)) void transposeToDouble(const T* v, double* out)
+{
+    for (uint32_t l = 0; l < 32; l++)
+        for (uint32_t k = 0; k < 4; k++) out[32 * k + l] = double(v[4 * l + k]);
+}
+
+double dist64(const uint8_t* x, const float* c)
+{
+    double xT[kDims], cT[kDims];
+    transposeToDouble(x, xT);
+    transposeToDouble(c, cT);
+    return dist64T(xT, cT);
+}
+
+// argmin over the B transposed centers cT[B][128], lowest index on ties.
+static inline __attribute__((always_inline)) uint32_t nearestT(const uint8_t* x, const double* cT, uint32_t B,
+                                                               double* dOut)
+{
+    double xT[kDims];
+    transposeToDouble(x, xT);
+    uint32_t best = 0;
+    double bestD = dist64T(xT, cT);
+    for (uint32_t b = 1; b < B; b++) {
+        const double d = dist64T(xT, cT + size_t(b) * kDims);
+        if (d < bestD) {
+            bestD = d;
+            best = b;
+        }
+    }
+    if (dOut) *dOut = bestD;
+    return best;
+}
+
+void transposeCenters(const float* c, uint32_t B, std::vector<double>& cT)
+{
+    cT.resize(size_t(B) * kDims);
+    for (uint32_t b = 0; b < B; b++) transposeToDouble(c + size_t(b) * kDims, cT.data() + size_t(b) * kDims);
+}
+
+// Nearest fp32 center (transposed cT[B][128]) of members[beg, end): assignment and distance.
+__attribute__((target_clones("avx512f", "fma", "default")))
+void assignRangeF(const uint8_t* desc, const uint32_t* members, uint32_t beg, uint32_t end, const double* cT,
+                  uint32_t B, uint8_t* next, double* dist)
+{
+    for (uint32_t i = beg; i < end; i++)
+        next[i] = static_cast<uint8_t>(nearestT(desc + size_t(members[i]) * kDims, cT, B, &dist[i]));
+}
+
+// Descent of desc[beg, end) through fp32 centers [levelBeg(L)][B][128].
+__attribute__((target_clones("avx512f", "fma", "default")))
+void lookupRangeF(const float* centers, uint32_t B, uint32_t L, const uint8_t* desc, uint64_t beg, uint64_t end,
+                  uint32_t* out)
+{
+    std::vector<double> cT(size_t(B) * kDims);
+    for (uint64_t i = beg; i < end; i++) {
+        const uint8_t* x = desc + i * kDims;
+        uint64_t idx = 0, lb = 0;
+        for (uint32_t level = 0; level < L; level++) {
+            const float* node = centers + (lb + idx) * B * kDims;
+            for (uint32_t b = 0; b < B; b++) transposeToDouble(node + size_t(b) * kDims, cT.data() + size_t(b) * kDims);
+            idx = idx * B + nearestT(x, cT.data(), B, nullptr);
+            lb = lb * B + 1;
+        }
+        out[i] = static_cast<uint32_t>(idx);
+    }
+}
+
+template <typename F>
+void parallelFor(uint64_t n, uint32_t nThreads, F&& f)
+{
+    if (nThreads <= 1 || n < 2) {
+        for (uint64_t i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::atomic<uint64_t> next{0};
+    std::vector<std::thread> pool;
+    const uint32_t m = static_cast<uint32_t>(std::min<uint64_t>(nThreads, n));
+    for (uint32_t t = 0; t < m; t++) {
+        pool.emplace_back([&] {
+            for (;;) {
+                const uint64_t i = next.fetch_add(1);
+                if (i >= n) break;
+                f(i);
+            }
+        });
+    }
+    for (auto& th : pool) th.join();
+}
+
+// Initial descriptor picks of every node of one level (the uint8 build's rules), in node order
+// because the reference init draws from one engine across the level.
+void levelInitPicks(uint32_t initMode, std::mt19937_64& rng, const uint8_t* desc,
+                    const std::vector<std::vector<uint32_t>>& groups, uint32_t B, uint64_t seed, uint32_t level,
+                    uint64_t lb, const uint32_t* injected, std::vector<uint32_t>& picks, std::vector<uint32_t>& nValid)
+{
+    const uint64_t nbGroups = groups.size();
+    picks.assign(nbGroups * B, kInvalid);
+    nValid.assign(nbGroups, 0u);
+    for (uint64_t g = 0; g < nbGroups; g++) {
+        const auto& members = groups[g];
+        const uint32_t n = static_cast<uint32_t>(members.size());
+        uint32_t* pk = picks.data() + g * B;
+        if (initMode == ORC_INIT_REFERENCE) {
+            std::vector<uint32_t> tmp(B);
+            nValid[g] = randPick(rng, tmp.data(), n, B);
+            if (n != 0) {
+                for (uint32_t b = 0; b < B; b++) pk[b] = members[tmp[b]];
+            } else {
+                uint32_t v = kInvalid;
+                for (uint64_t h = g + 1; h < nbGroups; h++) {
+                    if (!groups[h].empty()) {
+                        v = groups[h][0];
+                        break;
+                    }
+                }
+                for (uint32_t b = 0; b < B; b++) pk[b] = v;
+            }
+        } else if (initMode == ORC_INIT_KMEANSPP) {
+            nValid[g] = orc_kmeanspp_init(desc, members.data(), n, B, seed, level, g, pk);
+        } else {
+            for (uint32_t b = 0; b < B; b++) {
+                pk[b] = injected[(lb + g) * B + b];
+                if (pk[b] != kInvalid && b == nValid[g]) nValid[g]++;
+            }
+        }
+    }
+}
+
+struct NodeRunF {
+    uint32_t iters = 0;
+    double inertiaFirst = 0;
+    double inertiaLast = 0;
+};
+
+// Lloyd iterations of one node with fp32 centers (kmeans.cu:125-199 and 356-372 generalised,
+// freezing as kmeans.cu:238-240 / 341-343).  innerThreads > 1 splits the members' distances
+// over threads; every reduction is in member order, so the result does not depend on it.
+NodeRunF runNodeF(const uint8_t* desc, const std::vector<uint32_t>& members, uint32_t B, uint32_t maxIter, float* c,
+                  std::vector<uint8_t>& assign, uint32_t innerThreads)
+{
+    NodeRunF r;
+    const uint32_t n = static_cast<uint32_t>(members.size());
+    assign.assign(n, 0);
+    std::vector<uint8_t> next(n);
+    std::vector<double> dist(n);
+    std::vector<uint32_t> counts(B);
+    std::vector<uint64_t> sums(size_t(B) * kDims);
+    uint32_t last = 0xFFFFFFFFu;
+    constexpr uint32_t kChunk = 4096;
+    std::vector<double> cT;
+    for (uint32_t it = 0; it < maxIter; it++) {
+        uint32_t changed = 0;
+        if (last != 0) {
+            transposeCenters(c, B, cT);
+            parallelFor((n + kChunk - 1) / kChunk, innerThreads, [&](uint64_t ch) {
+                const uint32_t beg = static_cast<uint32_t>(ch * kChunk);
+                assignRangeF(desc, members.data(), beg, std::min(n, beg + kChunk), cT.data(), B, next.data(),
+                             dist.data());
+            });
+            std::fill(counts.begin(), counts.end(), 0u);
+            std::fill(sums.begin(), sums.end(), 0ull);
+            double inertia = 0.0;
+            for (uint32_t i = 0; i < n; i++) {
+                if (next[i] != assign[i]) changed++;
+                assign[i] = next[i];
+                counts[next[i]]++;
+                const uint8_t* x = desc + size_t(members[i]) * kDims;
+                uint64_t* s = sums.data() + size_t(next[i]) * kDims;
+                for (uint32_t k = 0; k < kDims; k++) s[k] += x[k];
+                inertia += dist[i];
+            }
+            if (it == 0) r.inertiaFirst = inertia;
+            r.inertiaLast = inertia;
+            r.iters = it + 1;
+        }
+        if (changed == 0) break;
+        for (uint32_t b = 0; b < B; b++) {
+            if (counts[b] == 0) continue;
+            for (uint32_t k = 0; k < kDims; k++)
+                c[size_t(b) * kDims + k] = float(double(sums[size_t(b) * kDims + k]) / double(counts[b]));
+        }
+        last = changed;
+    }
+    return r;
+}
+
+} // namespace
+
+extern "C" {
+
+double orc_dist64(const uint8_t* x, const float* c) { return dist64(x, c); }
+
+void orc_lookup_f32(const float* centers, uint32_t B, uint32_t L, const uint8_t* desc, uint64_t n, uint32_t* out,
+                    uint32_t nThreads)
+{
+    constexpr uint64_t kChunk = 2048;
+    parallelFor((n + kChunk - 1) / kChunk, nThreads, [&](uint64_t ch) {
+        const uint64_t beg = ch * kChunk;
+        lookupRangeF(centers, B, L, desc, beg, std::min(n, beg + kChunk), out);
+    });
+}
+
+int orc_build_vocabulary_f32(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, uint32_t B, uint32_t L,
+                             uint32_t maxIter, uint32_t initMode, uint64_t seed, const uint32_t* injected,
+                             float* centers, uint32_t* masks, float* weights, uint32_t* occ, uint32_t* itersOut,
+                             double* inertiaFirst, double* inertiaLast, uint32_t nThreads)
+{
+    if (nbDesc < B || nbDoc == 0 || B < 2 || B > 16) return -1;
+    const uint64_t nbNodes = levelBeg(B, L);
+    std::fill(masks, masks + nbNodes, 0u);
+    std::fill(occ, occ + nbNodes * B, 0u);
+    std::mt19937_64 rng{};
+    std::vector<std::vector<uint32_t>> groups{std::vector<uint32_t>(nbDesc)};
+    std::iota(groups[0].begin(), groups[0].end(), 0u);
+    std::vector<uint32_t> picks, nValid;
+    for (uint32_t level = 0; level < L; level++) {
+        const uint64_t lb = levelBeg(B, level);
+        const uint64_t nbGroups = groups.size();
+        levelInitPicks(initMode, rng, desc, groups, B, seed, level, lb, injected, picks, nValid);
+        for (uint64_t g = 0; g < nbGroups; g++) {
+            float* c = centers + (lb + g) * B * kDims;
+            for (uint32_t b = 0; b < B; b++) {
+                const uint32_t pk = picks[g * B + b];
+                for (uint32_t k = 0; k < kDims; k++)
+                    c[size_t(b) * kDims + k] = pk == kInvalid ? 255.0f : float(desc[size_t(pk) * kDims + k]);
+            }
+            masks[lb + g] = nValid[g] >= 32 ? 0xFFFFFFFFu : ((1u << nValid[g]) - 1u);
+        }
+        std::vector<NodeRunF> runs(nbGroups);
+        std::vector<std::vector<uint8_t>> assigns(nbGroups);
+        const bool manyNodes = nbGroups >= 4ull * std::max(1u, nThreads);
+        parallelFor(nbGroups, manyNodes ? nThreads : 1u, [&](uint64_t g) {
+            runs[g] = runNodeF(desc, groups[g], B, maxIter, centers + (lb + g) * B * kDims, assigns[g],
+                               manyNodes ? 1u : nThreads);
+        });
+        double first = 0.0, lastSum = 0.0;
+        std::vector<std::vector<uint32_t>> next(nbGroups * B);
+        for (uint64_t g = 0; g < nbGroups; g++) {
+            first += runs[g].inertiaFirst;
+            lastSum += runs[g].inertiaLast;
+            if (itersOut) itersOut[lb + g] = runs[g].iters;
+            const auto& members = groups[g];
+            for (size_t i = 0; i < members.size(); i++) next[g * B + assigns[g][i]].push_back(members[i]);
+            for (uint32_t b = 0; b < B; b++) occ[(lb + g) * B + b] = static_cast<uint32_t>(next[g * B + b].size());
+        }
+        if (inertiaFirst) inertiaFirst[level] = first;
+        if (inertiaLast) inertiaLast[level] = lastSum;
+        groups.swap(next);
+    }
     for (uint64_t i = 0; i < nbNodes * B; i++) {
         weights[i] = occ[i] == 0 ? std::numeric_limits<float>::min()
                                  : std::max(std::numeric_limits<float>::min(),

@@ -61,6 +61,32 @@ int orc_build_vocabulary(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, u
                          uint32_t maxIter, uint32_t initMode, uint64_t seed, const uint32_t* injected,
                          uint8_t* centers, uint32_t* masks, float* weights, uint32_t* occ, uint32_t* itersOut);
 
+/* ---- Float-center mode (no counterpart in the reference, whose centers are uint8: kmeans.cu:367).
+ * It generalises the reference's assign/update (kmeans.cu:125-199, 356-372) to fp32 centers:
+ *   distance : FP64 squared L2 in one fixed evaluation order, identical on the GPU (orc_dist64);
+ *   assign   : argmin of that distance, lowest index on ties (kmeans.cu:131-135);
+ *   update   : c = float(double(sum) / double(count)) from exact integer sums, kept when count = 0;
+ *   inertia  : FP64 sum over the members of their distance to the assigned center.
+ * Initial centers are the same descriptor rows as in the uint8 mode (converted exactly). */
+
+/* Squared distance of a uint8 row to an fp32 center: lane l (0..31) forms
+ * p_l = fma(e, e, .) over e = double(x[4l+k]) - double(c[4l+k]), k = 0..3 (starting from 0);
+ * then for off = 16, 8, 4, 2, 1: p_l = p_l + p_(l xor off); the result is p_0. */
+double orc_dist64(const uint8_t* x, const float* c);
+
+/* Tree descent through fp32 centers [levelBeg(L)][B][128] with orc_dist64. */
+void orc_lookup_f32(const float* centers, uint32_t B, uint32_t L, const uint8_t* desc, uint64_t n,
+                    uint32_t* out, uint32_t nThreads);
+
+/* Float-center hierarchical build, same level loop, init modes and freezing rule as
+ * orc_build_vocabulary.  centers: float [levelBeg(L)][B][128].  inertiaFirst / inertiaLast
+ * [L]: the level's inertia (sum over its nodes) after its first and after its last Lloyd step
+ * (frozen nodes keep their last value); either may be NULL. */
+int orc_build_vocabulary_f32(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, uint32_t B, uint32_t L,
+                             uint32_t maxIter, uint32_t initMode, uint64_t seed, const uint32_t* injected,
+                             float* centers, uint32_t* masks, float* weights, uint32_t* occ, uint32_t* itersOut,
+                             double* inertiaFirst, double* inertiaLast, uint32_t nThreads);
+
 /* Inverted file + scoring (DataBase.cpp:39-197), B = branching, L = levels. */
 void* orc_db_create(uint32_t B, uint32_t L, const float* weights);
 void orc_db_destroy(void* db);

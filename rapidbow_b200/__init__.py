@@ -48,6 +48,15 @@ class BuildOptions(C.Structure):
                 ("flags", C.c_uint32), ("seed", C.c_uint64), ("injected_init", C.c_void_p)]
 
 
+class BuildStats(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("iterations", C.c_uint32 * 16), ("inertia_first", C.c_double * 16),
+                ("inertia_last", C.c_double * 16), ("refined", C.c_uint64 * 16), ("assignments", C.c_uint64 * 16),
+                ("seconds", C.c_double)]
+
+
+BUILD_IEEE_DIVISION, BUILD_FLOAT_CENTERS = 1, 2
+
+
 class RbwError(RuntimeError):
     def __init__(self, status: int, message: str) -> None:
         super().__init__(message)
@@ -85,6 +94,11 @@ def load_library() -> C.CDLL:
         "rbw_voc_device_errors": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
         "rbw_voc_destroy": (None, [vp]),
         "rbw_voc_lookup_noalloc": (C.c_int, [vp, vp, u32, vp, vp]),
+        "rbw_voc_from_host_f32": (C.c_int, [u32, u32, vp, vp, vp, pp]),
+        "rbw_voc_center_type": (C.c_int, [vp, C.POINTER(i32)]),
+        "rbw_voc_get_centers_f32": (C.c_int, [vp, vp]),
+        "rbw_voc_build_stats": (C.c_int, [vp, C.POINTER(BuildStats)]),
+        "rbw_voc_refined_lookups": (C.c_int, [vp, C.POINTER(u64)]),
         "rbw_timing_enable": (None, [i32]),
         "rbw_timing_reset": (C.c_int, []),
         "rbw_timing_read": (C.c_int, [u32, C.POINTER(C.c_double), C.POINTER(u64)]),
@@ -201,6 +215,34 @@ class Vocabulary:
         n = (B ** level) * B
         return np.ctypeslib.as_array(p, shape=(n,)).reshape(B ** level, B).copy()
 
+    @property
+    def float_centers(self) -> bool:
+        """True for a float-center vocabulary (RBW_CENTERS_FLOAT32)."""
+        v = C.c_int32()
+        _check(self._lib.rbw_voc_center_type(self._h, C.byref(v)))
+        return v.value == 1
+
+    def centers_f32(self) -> np.ndarray:
+        """fp32 centers [nodes][B][128] of a float-center vocabulary."""
+        c = np.empty((self.nb_nodes, self.branch_factor, 128), np.float32)
+        _check(self._lib.rbw_voc_get_centers_f32(self._h, c.ctypes.data))
+        return c
+
+    def build_stats(self) -> dict:
+        """Statistics of the build (iterations, FP64 inertia, FP64 re-scored assignments per level)."""
+        s = BuildStats()
+        _check(self._lib.rbw_voc_build_stats(self._h, C.byref(s)))
+        L = s.levels
+        return {"levels": L, "iterations": list(s.iterations[:L]), "inertia_first": list(s.inertia_first[:L]),
+                "inertia_last": list(s.inertia_last[:L]), "refined": list(s.refined[:L]),
+                "assignments": list(s.assignments[:L]), "seconds": s.seconds}
+
+    def refined_lookups(self) -> int:
+        """Lookup descriptors re-scored in FP64 since the last call (float centers)."""
+        v = C.c_uint64()
+        _check(self._lib.rbw_voc_refined_lookups(self._h, C.byref(v)))
+        return v.value
+
     def tree(self):
         """(centers [nodes][B][128] uint8, masks [nodes] uint32, weights [nodes][B] float32)."""
         B, nodes = self.branch_factor, self.nb_nodes
@@ -293,10 +335,11 @@ def timing_read(kernel: str):
 def build_vocabulary(descriptors, branch_factor: int = 16, nb_doc: int = 1, nb_levels: int = 4, stream=None,
                      max_iterations: int = 1000, check_interval: int = 4, init: str = "reference", seed: int = 0,
                      injected: Optional[np.ndarray] = None, attr=SIFT_ATTR,
-                     ieee_division: bool = False) -> Vocabulary:
+                     ieee_division: bool = False, float_centers: bool = False) -> Vocabulary:
     """rbow::buildVocabulary (RapidBoW.h:82-88); descriptors is a CUDA uint8 tensor [n, 128].
     ieee_division=True rounds centers with the correctly rounded quotient instead of the
-    reference's fast-math division."""
+    reference's fast-math division; float_centers=True keeps fp32 centers (split-bf16 distances
+    with an FP64 re-score near ties, see RBW_BUILD_FLOAT_CENTERS)."""
     lib = load_library()
     o = BuildOptions()
     lib.rbw_build_options_default(C.byref(o))
@@ -304,7 +347,7 @@ def build_vocabulary(descriptors, branch_factor: int = 16, nb_doc: int = 1, nb_l
     o.check_interval = check_interval
     o.init_mode = INIT_MODES[init]
     o.seed = seed
-    o.flags = 1 if ieee_division else 0
+    o.flags = (BUILD_IEEE_DIVISION if ieee_division else 0) | (BUILD_FLOAT_CENTERS if float_centers else 0)
     keep = None
     if injected is not None:
         keep = np.ascontiguousarray(injected, dtype=np.uint32)
@@ -326,6 +369,19 @@ def vocabulary_from_host(branch_factor: int, nb_levels: int, centers: np.ndarray
     h = C.c_void_p()
     _check(lib.rbw_voc_from_host(branch_factor, nb_levels, centers.ctypes.data, masks.ctypes.data,
                                  weights.ctypes.data, C.byref(h)))
+    return Vocabulary(h.value)
+
+
+def vocabulary_from_host_f32(branch_factor: int, nb_levels: int, centers: np.ndarray, masks: np.ndarray,
+                             weights: np.ndarray) -> Vocabulary:
+    """A float-center vocabulary from fp32 centers [nodes][B][128]."""
+    lib = load_library()
+    centers = np.ascontiguousarray(centers, dtype=np.float32)
+    masks = np.ascontiguousarray(masks, dtype=np.uint32)
+    weights = np.ascontiguousarray(weights, dtype=np.float32)
+    h = C.c_void_p()
+    _check(lib.rbw_voc_from_host_f32(branch_factor, nb_levels, centers.ctypes.data, masks.ctypes.data,
+                                     weights.ctypes.data, C.byref(h)))
     return Vocabulary(h.value)
 
 

@@ -24,7 +24,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
 # Per-file extra flags: the center update must divide exactly like the reference's
 # --use_fast_math kernels.
 EXTRA = {"kmeans_update.cu": ["--use_fast_math"]}
-SOURCES = ["lookup.cu", "kmeans.cu", "kmeans_update.cu", "vocabulary.cu", "database.cu", "capi.cpp", "facade.cpp",
+SOURCES = ["lookup.cu", "kmeans.cu", "kmeans_update.cu", "kmeans_f32.cu", "vocabulary.cu", "database.cu", "capi.cpp", "facade.cpp",
            "timing.cpp", "noalloc.cu", "server.cpp"]
 
 

@@ -80,6 +80,9 @@ int rbw_voc_build(rbw_desc_attr attr, uint32_t branch_factor, const void* dev_de
             o.seed = opts->seed;
             o.injected = opts->injected_init;
             o.ieeeDivision = (opts->flags & RBW_BUILD_IEEE_DIVISION) != 0;
+            o.floatCenters = (opts->flags & RBW_BUILD_FLOAT_CENTERS) != 0;
+            if (opts->flags & ~uint32_t(RBW_BUILD_IEEE_DIVISION | RBW_BUILD_FLOAT_CENTERS))
+                throw rbw::Error(rbw::kInvalidArg, "unknown build flag");
             if (o.initMode > rbw::kInitInjected) throw rbw::Error(rbw::kInvalidArg, "unknown init mode");
         }
         auto v = rbw::Vocabulary::build(branch_factor, nb_levels, static_cast<const uint8_t*>(dev_desc), nb_desc,
@@ -97,6 +100,62 @@ int rbw_voc_from_host(uint32_t branch_factor, uint32_t nb_levels, const uint8_t*
         *out = nullptr;
         auto v = rbw::Vocabulary::fromHost(branch_factor, nb_levels, centers, masks, weights);
         *out = new rbw_vocabulary{std::move(v)};
+    });
+}
+
+int rbw_voc_from_host_f32(uint32_t branch_factor, uint32_t nb_levels, const float* centers, const uint32_t* masks,
+                          const float* weights, rbw_vocabulary** out)
+{
+    return guard([&] {
+        if (out == nullptr || centers == nullptr || masks == nullptr || weights == nullptr)
+            throw rbw::Error(rbw::kInvalidArg, "null argument");
+        *out = nullptr;
+        auto v = rbw::Vocabulary::fromHostF32(branch_factor, nb_levels, centers, masks, weights);
+        *out = new rbw_vocabulary{std::move(v)};
+    });
+}
+
+int rbw_voc_center_type(const rbw_vocabulary* voc, int32_t* type)
+{
+    return guard([&] {
+        if (type == nullptr) throw rbw::Error(rbw::kInvalidArg, "null output");
+        *type = vocOf(voc).floatCenters() ? RBW_CENTERS_FLOAT32 : RBW_CENTERS_UINT8;
+    });
+}
+
+int rbw_voc_get_centers_f32(const rbw_vocabulary* voc, float* host_centers)
+{
+    return guard([&] {
+        if (host_centers == nullptr) throw rbw::Error(rbw::kInvalidArg, "null output");
+        const auto c = vocOf(voc).centersF32Host();
+        std::memcpy(host_centers, c.data(), c.size() * sizeof(float));
+    });
+}
+
+int rbw_voc_build_stats(const rbw_vocabulary* voc, rbw_build_stats* stats)
+{
+    return guard([&] {
+        if (stats == nullptr) throw rbw::Error(rbw::kInvalidArg, "null output");
+        const rbw::BuildStats& s = vocOf(voc).buildStats();
+        std::memset(stats, 0, sizeof(*stats));
+        stats->levels = s.levels;
+        for (int i = 0; i < 16; i++) {
+            stats->iterations[i] = s.iterations[i];
+            stats->inertia_first[i] = s.inertiaFirst[i];
+            stats->inertia_last[i] = s.inertiaLast[i];
+            stats->refined[i] = s.refined[i];
+            stats->assignments[i] = s.assignments[i];
+        }
+        stats->seconds = s.seconds;
+    });
+}
+
+int rbw_voc_refined_lookups(const rbw_vocabulary* voc, uint64_t* refined)
+{
+    return guard([&] {
+        if (refined == nullptr) throw rbw::Error(rbw::kInvalidArg, "null output");
+        RBW_CUDA(cudaDeviceSynchronize());
+        *refined = vocOf(voc).takeRefinedLookups();
     });
 }
 

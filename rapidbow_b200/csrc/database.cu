@@ -45,12 +45,12 @@
 namespace rbw {
 namespace {
 
-constexpr uint32_t kMaxDocDesc = 32768;   // descriptors per document or query (in-CTA sort)
+constexpr uint32_t kMaxDocDesc = 32768;   // descriptors sorted in shared memory; larger ones in global memory
 constexpr uint32_t kPrepThreads = 512;
 constexpr uint32_t kScoreThreads = 1024;
 constexpr uint32_t kSegThreads = 256;
 constexpr uint32_t kSmemDocs = 20480;     // per-document accumulators kept in shared memory
-constexpr uint32_t kMaxK = 1024;
+constexpr uint32_t kMaxK = 1024;          // results selected in shared memory; more in global memory
 constexpr double kFixScale = 72057594037927936.0; // 2^56
 constexpr uint32_t kDeltaMinDocs = 256;   // the delta may always hold this many documents
 constexpr uint32_t kDeltaFraction = 4;    // ... or up to main / kDeltaFraction
@@ -156,20 +156,25 @@ __device__ double l1NormWarp(const uint32_t* sorted, uint32_t n, const float* we
 }
 
 // ------------------------------------------------------------------ documents
-// One CTA per new document (slot s0 + blockIdx.x).  newLeaves holds the new documents' leaves
-// back to back, starting at posting offset docOff[s0].
+// One CTA per new document.  newLeaves holds the new documents' leaves back to back, starting at
+// posting offset docOff[s0].  Without gkeys, CTA i prepares slot s0 + i in shared memory and
+// skips documents above kMaxDocDesc descriptors; with gkeys, CTA i prepares slot slotList[i],
+// sorting in its gstride-word slice of gkeys.
 __global__ void __launch_bounds__(kPrepThreads) docPrepKernel(const uint32_t* newLeaves, const uint64_t* docOff,
-                                                              uint32_t s0, const float* weights, uint32_t B,
+                                                              uint32_t s0, const uint32_t* slotList, uint32_t* gkeys,
+                                                              uint32_t gstride, const float* weights, uint32_t B,
                                                               uint32_t L, uint64_t nbLeaves, float* rcpF,
                                                               uint64_t* docPairs, uint32_t* pairCount)
 {
-    extern __shared__ uint32_t keys[];
+    extern __shared__ uint32_t skeys[];
     __shared__ uint32_t cnt, nValid;
-    const uint32_t slot = s0 + blockIdx.x;
+    const uint32_t slot = gkeys ? slotList[blockIdx.x] : s0 + blockIdx.x;
     const uint64_t beg = docOff[slot];
+    const uint32_t nAll = static_cast<uint32_t>(docOff[slot + 1] - beg);
+    if (gkeys == nullptr && nAll > kMaxDocDesc) return; // prepared by the global-memory launch
+    uint32_t* keys = gkeys ? gkeys + uint64_t(blockIdx.x) * gstride : skeys;
     if (threadIdx.x == 0) cnt = 0;
-    const uint32_t n = loadAndSort(newLeaves + (beg - docOff[s0]), static_cast<uint32_t>(docOff[slot + 1] - beg),
-                                   keys, nbLeaves, &nValid);
+    const uint32_t n = loadAndSort(newLeaves + (beg - docOff[s0]), nAll, keys, nbLeaves, &nValid);
     if (threadIdx.x < 32) {
         const double norm = l1NormWarp(keys, n, weights, B, L);
         if (threadIdx.x == 0) rcpF[slot] = float(1 / norm); // DataBase.cpp:68
@@ -247,19 +252,26 @@ __global__ void wordPostKernel(unsigned long long* wordPost, uint32_t B, uint32_
 }
 
 // ------------------------------------------------------------------ queries
+// One CTA per query: without gkeys CTA i prepares query i in shared memory (skipping queries
+// above kMaxDocDesc descriptors); with gkeys CTA i prepares query qList[i] in its gstride-word
+// slice of gkeys.
 __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* qLeaves, const uint64_t* qOff,
-                                                                const float* weights,
+                                                                const uint32_t* qList, uint32_t* gkeys,
+                                                                uint32_t gstride, const float* weights,
                                                                 const unsigned long long* wordPost, uint32_t B,
                                                                 uint32_t L, uint64_t nbLeaves, uint32_t k,
                                                                 float* qRcpF, Entry* entries, uint32_t* entryCount)
 {
-    extern __shared__ uint32_t keys[];
+    extern __shared__ uint32_t skeys[];
     __shared__ uint32_t cnt, nValid;
-    const uint32_t q = blockIdx.x;
+    const uint32_t q = gkeys ? qList[blockIdx.x] : blockIdx.x;
     const uint64_t beg = qOff[q];
+    const uint32_t nAll = static_cast<uint32_t>(qOff[q + 1] - beg);
+    if (gkeys == nullptr && nAll > kMaxDocDesc) return; // prepared by the global-memory launch
+    uint32_t* keys = gkeys ? gkeys + uint64_t(blockIdx.x) * gstride : skeys;
     Entry* out = entries + (beg - qOff[0]) * L;
     if (threadIdx.x == 0) cnt = 0;
-    const uint32_t n = loadAndSort(qLeaves + beg, static_cast<uint32_t>(qOff[q + 1] - beg), keys, nbLeaves, &nValid);
+    const uint32_t n = loadAndSort(qLeaves + beg, nAll, keys, nbLeaves, &nValid);
     if (threadIdx.x < 32) {
         const double norm = l1NormWarp(keys, n, weights, B, L);
         if (threadIdx.x == 0) qRcpF[q] = float(1 / norm); // DataBase.cpp:77-94
@@ -315,6 +327,8 @@ struct ScoreParams {
     uint32_t L;
     uint32_t k;
     unsigned long long* cand;  // [nq][shards][k] candidate keys when there are several shards
+    unsigned long long* selGlobal; // k > kMaxK: [nq][shards][selStride] selection buffers
+    uint32_t selStride;        // power of two >= k
     uint32_t* outDocs;         // [nq][k]
     float* outScores;          // [nq][k]
     uint32_t* outCount;        // [nq]
@@ -343,8 +357,10 @@ __device__ __forceinline__ float fromOrderedBits(uint32_t o)
 
 // The `want` smallest of n distinct keys (~0 = no key), ascending, into sel[0, want): radix
 // select of the want-th smallest key, 8 bits at a time, then a bitonic sort of the winners.
-// All threads of the CTA call it; keys may live in shared or global memory.
-__device__ __forceinline__ void selectSmallest(const unsigned long long* keys, uint32_t n, uint32_t want, unsigned long long* sel)
+// All threads of the CTA call it; keys and sel may live in shared or global memory; selCap is a
+// power of two >= want.
+__device__ __forceinline__ void selectSmallest(const unsigned long long* keys, uint32_t n, uint32_t want,
+                                               unsigned long long* sel, uint32_t selCap)
 {
     __shared__ uint32_t hist[256];
     __shared__ unsigned long long prefix;
@@ -381,12 +397,12 @@ __device__ __forceinline__ void selectSmallest(const unsigned long long* keys, u
             const unsigned long long key = keys[i];
             if (key <= prefix) {
                 const uint32_t s = atomicAdd(&nSel, 1u);
-                if (s < kMaxK) sel[s] = key;
+                if (s < selCap) sel[s] = key;
             }
         }
     }
     __syncthreads();
-    const uint32_t m = nSel < kMaxK ? nSel : kMaxK;
+    const uint32_t m = nSel < selCap ? nSel : selCap;
     uint32_t mPow2 = 1;
     while (mPow2 < m) mPow2 <<= 1;
     for (uint32_t i = m + threadIdx.x; i < mPow2; i += blockDim.x) sel[i] = ~0ull;
@@ -524,12 +540,13 @@ __global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
     atomicAdd(&nTouched, myTouched);
     __syncthreads();
     const uint32_t want = P.k < nTouched ? P.k : nTouched;
-    selectSmallest(acc, nLocal, want, sel);
+    unsigned long long* selp = P.selGlobal ? P.selGlobal + (uint64_t(q) * gridDim.y + shard) * P.selStride : sel;
+    selectSmallest(acc, nLocal, want, selp, P.selGlobal ? P.selStride : kMaxK);
     if (P.cand == nullptr) {
-        writeResults(P, q, sel, want);
+        writeResults(P, q, selp, want);
     } else {
         unsigned long long* c = P.cand + (uint64_t(q) * gridDim.y + shard) * P.k;
-        for (uint32_t i = threadIdx.x; i < P.k; i += blockDim.x) c[i] = i < want ? sel[i] : ~0ull;
+        for (uint32_t i = threadIdx.x; i < P.k; i += blockDim.x) c[i] = i < want ? selp[i] : ~0ull;
     }
 }
 
@@ -548,8 +565,9 @@ __global__ void __launch_bounds__(kScoreThreads) mergeKernel(ScoreParams P, uint
     atomicAdd(&nValid, mine);
     __syncthreads();
     const uint32_t want = P.k < nValid ? P.k : nValid;
-    selectSmallest(c, n, want, sel);
-    writeResults(P, q, sel, want);
+    unsigned long long* selp = P.selGlobal ? P.selGlobal + uint64_t(q) * shards * P.selStride : sel;
+    selectSmallest(c, n, want, selp, P.selGlobal ? P.selStride : kMaxK);
+    writeResults(P, q, selp, want);
 }
 
 // Device memory from the library's stream-ordered pool, grown on a stream (keeping a prefix).
@@ -649,8 +667,8 @@ public:
         // validate the whole batch first: a failed call adds nothing
         std::unordered_map<uint32_t, uint32_t> seen;
         for (uint32_t d = 0; d < nDocs; d++) {
-            if (off[d + 1] < off[d] || off[d + 1] - off[d] > kMaxDocDesc)
-                throw Error(kInvalidArg, "bad document offsets or document too large");
+            if (off[d + 1] < off[d] || off[d + 1] - off[d] > 0xFFFFFFFFull)
+                throw Error(kInvalidArg, "bad document offsets");
             checkDoc(ids[d], leaves + off[d], static_cast<uint32_t>(off[d + 1] - off[d]));
             if (!seen.emplace(ids[d], d).second) throw Error(kDuplicate, "Duplicate document index");
         }
@@ -661,8 +679,6 @@ public:
     // Host leaves in, host results out (the reference's query).  Synchronous.
     uint32_t query(const uint32_t* leaves, uint32_t n, uint32_t k, uint32_t* docs, float* scores)
     {
-        if (n > kMaxDocDesc) throw Error(kUnsupported, "a query may hold at most 32768 descriptors");
-        if (k > kMaxK) throw Error(kUnsupported, "maxNbResults above 1024 is not supported");
         for (uint32_t i = 0; i < n; i++)
             if (leaves[i] >= mNbLeaves) throw Error(kInvalidArg, "leaf index out of range");
         if (k == 0) return 0;
@@ -705,7 +721,6 @@ public:
     void queryBatched(const uint32_t* dLeaves, const uint64_t* dOff, uint32_t nq, uint32_t k, uint32_t* dDocs,
                       float* dScores, uint32_t* dCount, cudaStream_t stream, const uint64_t* hostOff = nullptr)
     {
-        if (k > kMaxK) throw Error(kUnsupported, "maxNbResults above 1024 is not supported");
         if (nq == 0) return;
         if (dOff == nullptr || dCount == nullptr || (k && (dDocs == nullptr || dScores == nullptr)))
             throw Error(kInvalidArg, "null argument");
@@ -716,13 +731,20 @@ public:
             RBW_CUDA(cudaStreamSynchronize(stream));
             hostOff = off.data();
         }
-        uint32_t maxN = 0;
+        uint32_t maxN = 0, maxBig = 0;
+        std::vector<uint32_t> bigQ; // queries sorted in global memory
         for (uint32_t q = 0; q < nq; q++) {
-            if (hostOff[q + 1] < hostOff[q] || hostOff[q + 1] - hostOff[q] > kMaxDocDesc)
-                throw Error(kInvalidArg, "bad query offsets or query above 32768 descriptors");
-            maxN = std::max<uint32_t>(maxN, static_cast<uint32_t>(hostOff[q + 1] - hostOff[q]));
+            if (hostOff[q + 1] < hostOff[q] || hostOff[q + 1] - hostOff[q] > 0xFFFFFFFFull)
+                throw Error(kInvalidArg, "bad query offsets");
+            const uint32_t m = static_cast<uint32_t>(hostOff[q + 1] - hostOff[q]);
+            if (m > kMaxDocDesc) {
+                bigQ.push_back(q);
+                maxBig = std::max(maxBig, m);
+            } else {
+                maxN = std::max(maxN, m);
+            }
         }
-        if (maxN && dLeaves == nullptr) throw Error(kInvalidArg, "null argument");
+        if ((maxN || maxBig) && dLeaves == nullptr) throw Error(kInvalidArg, "null argument");
         const uint64_t totalLeaves = hostOff[nq] - hostOff[0];
         updateIndex();
         std::shared_lock<std::shared_mutex> lk(mMu);
@@ -737,19 +759,36 @@ public:
         const uint32_t shards = std::max(1u, (nDocs + shardDocs - 1) / shardDocs);
         const size_t entBytes = std::max<uint64_t>(totalLeaves, 1) * mL * sizeof(Entry);
         const size_t candBytes = shards > 1 ? size_t(nq) * shards * k * 8 : 16;
-        void *ent = nullptr, *cnt = nullptr, *qr = nullptr, *cand = nullptr;
+        const uint32_t selStride = k > kMaxK ? nextPow2(k) : 0u;
+        const size_t selBytes = k > kMaxK ? size_t(nq) * shards * selStride * 8 : 16;
+        const uint32_t bigStride = maxBig ? nextPow2(maxBig) : 0u;
+        const size_t bigBytes = bigQ.empty() ? 16 : bigQ.size() * (size_t(bigStride) + 1) * 4;
+        void *ent = nullptr, *cnt = nullptr, *qr = nullptr, *cand = nullptr, *selG = nullptr, *big = nullptr;
         RBW_CUDA(cudaMallocFromPoolAsync(&ent, entBytes, pool, stream));
         RBW_CUDA(cudaMallocFromPoolAsync(&cnt, size_t(nq) * 4, pool, stream));
         RBW_CUDA(cudaMallocFromPoolAsync(&qr, size_t(nq) * 4, pool, stream));
         RBW_CUDA(cudaMallocFromPoolAsync(&cand, candBytes, pool, stream));
+        RBW_CUDA(cudaMallocFromPoolAsync(&selG, selBytes, pool, stream));
+        RBW_CUDA(cudaMallocFromPoolAsync(&big, bigBytes, pool, stream));
         {
             ScopedKernelTimer timer(kTimedScore, stream);
             const size_t prepSmem = size_t(nextPow2(std::max(maxN, 1u))) * 4;
             RBW_CUDA(cudaFuncSetAttribute(queryPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(prepSmem)));
             queryPrepKernel<<<nq, kPrepThreads, prepSmem, stream>>>(
-                dLeaves, dOff, mWeights.as<float>(), mWordPost.as<unsigned long long>(), mB, mL, mNbLeaves, k,
-                static_cast<float*>(qr), static_cast<Entry*>(ent), static_cast<uint32_t*>(cnt));
+                dLeaves, dOff, nullptr, nullptr, 0u, mWeights.as<float>(), mWordPost.as<unsigned long long>(), mB, mL,
+                mNbLeaves, k, static_cast<float*>(qr), static_cast<Entry*>(ent), static_cast<uint32_t*>(cnt));
             RBW_CUDA(cudaGetLastError());
+            if (!bigQ.empty()) {
+                // queries above kMaxDocDesc descriptors: one CTA each, sorted in global memory
+                uint32_t* qList = static_cast<uint32_t*>(big);
+                uint32_t* gkeys = qList + bigQ.size();
+                RBW_CUDA(cudaMemcpyAsync(qList, bigQ.data(), bigQ.size() * 4, cudaMemcpyHostToDevice, stream));
+                queryPrepKernel<<<static_cast<uint32_t>(bigQ.size()), kPrepThreads, 0, stream>>>(
+                    dLeaves, dOff, qList, gkeys, bigStride, mWeights.as<float>(), mWordPost.as<unsigned long long>(),
+                    mB, mL, mNbLeaves, k, static_cast<float*>(qr), static_cast<Entry*>(ent),
+                    static_cast<uint32_t*>(cnt));
+                RBW_CUDA(cudaGetLastError());
+            }
             ScoreParams P{};
             P.entries = static_cast<const Entry*>(ent);
             P.entryCount = static_cast<const uint32_t*>(cnt);
@@ -767,6 +806,8 @@ public:
             P.L = mL;
             P.k = k;
             P.cand = shards > 1 ? static_cast<unsigned long long*>(cand) : nullptr;
+            P.selGlobal = k > kMaxK ? static_cast<unsigned long long*>(selG) : nullptr;
+            P.selStride = selStride;
             P.outDocs = dDocs;
             P.outScores = dScores;
             P.outCount = dCount;
@@ -788,6 +829,8 @@ public:
         RBW_CUDA(cudaFreeAsync(cnt, stream));
         RBW_CUDA(cudaFreeAsync(qr, stream));
         RBW_CUDA(cudaFreeAsync(cand, stream));
+        RBW_CUDA(cudaFreeAsync(selG, stream));
+        RBW_CUDA(cudaFreeAsync(big, stream));
         recordQuery(stream);
     }
 
@@ -845,7 +888,7 @@ public:
                 RBW_CUDA(cudaStreamSynchronize(mStream));
             }
             for (size_t i = 0; i < pr.size(); i++) {
-                if (tf[i] > kMaxDocDesc || (pr[i] >> 32) >= mHostIds.size())
+                if (tf[i] > mHostDocOff.back() || (pr[i] >> 32) >= mHostIds.size())
                     throw Error(kInternal, "inconsistent posting entry");
                 out.insert(out.end(), tf[i], mHostIds[pr[i] >> 32]);
             }
@@ -858,7 +901,6 @@ private:
     void checkDoc(uint32_t id, const uint32_t* leaves, uint32_t n) const
     {
         if (mSlotOf.count(id)) throw Error(kDuplicate, "Duplicate document index"); // DataBase.cpp:41-43
-        if (n > kMaxDocDesc) throw Error(kUnsupported, "a document may hold at most 32768 descriptors");
         if (n && leaves == nullptr) throw Error(kInvalidArg, "null leaves");
         for (uint32_t i = 0; i < n; i++)
             if (leaves[i] >= mNbLeaves) throw Error(kInvalidArg, "leaf index out of range");
@@ -870,7 +912,7 @@ private:
         mHostIds.push_back(id);
         mStage.insert(mStage.end(), leaves, leaves + n);
         mHostDocOff.push_back(mHostDocOff.back() + n);
-        mStageMaxN = std::max(mStageMaxN, n);
+        if (n <= kMaxDocDesc) mStageMaxN = std::max(mStageMaxN, n);
     }
 
     // Makes the stream wait for every query launched since the last index update.
@@ -960,9 +1002,33 @@ private:
         const size_t smem = size_t(nextPow2(std::max(mStageMaxN, 1u))) * 4;
         RBW_CUDA(cudaFuncSetAttribute(docPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         docPrepKernel<<<s1 - s0, kPrepThreads, smem, mStream>>>(
-            static_cast<const uint32_t*>(newLeaves), mDocOff.as<uint64_t>(), s0, mWeights.as<float>(), mB, mL,
-            mNbLeaves, mRcpF.as<float>(), mDocPairs.as<uint64_t>(), mPairCount.as<uint32_t>());
+            static_cast<const uint32_t*>(newLeaves), mDocOff.as<uint64_t>(), s0, nullptr, nullptr, 0u,
+            mWeights.as<float>(), mB, mL, mNbLeaves, mRcpF.as<float>(), mDocPairs.as<uint64_t>(),
+            mPairCount.as<uint32_t>());
         RBW_CUDA(cudaGetLastError());
+        // documents above kMaxDocDesc descriptors: one CTA each, sorted in global memory
+        std::vector<uint32_t> bigSlots;
+        uint64_t maxBig = 0;
+        for (uint32_t s = s0; s < s1; s++) {
+            const uint64_t m = mHostDocOff[s + 1] - mHostDocOff[s];
+            if (m > kMaxDocDesc) {
+                bigSlots.push_back(s);
+                maxBig = std::max(maxBig, m);
+            }
+        }
+        if (!bigSlots.empty()) {
+            const uint32_t stride = nextPow2(static_cast<uint32_t>(maxBig));
+            void* big = nullptr;
+            RBW_CUDA(cudaMallocFromPoolAsync(&big, bigSlots.size() * (size_t(stride) + 1) * 4, libraryPool(), mStream));
+            uint32_t* slotList = static_cast<uint32_t*>(big);
+            RBW_CUDA(cudaMemcpyAsync(slotList, bigSlots.data(), bigSlots.size() * 4, cudaMemcpyHostToDevice, mStream));
+            docPrepKernel<<<static_cast<uint32_t>(bigSlots.size()), kPrepThreads, 0, mStream>>>(
+                static_cast<const uint32_t*>(newLeaves), mDocOff.as<uint64_t>(), s0, slotList,
+                slotList + bigSlots.size(), stride, mWeights.as<float>(), mB, mL, mNbLeaves, mRcpF.as<float>(),
+                mDocPairs.as<uint64_t>(), mPairCount.as<uint32_t>());
+            RBW_CUDA(cudaGetLastError());
+            RBW_CUDA(cudaFreeAsync(big, mStream));
+        }
         RBW_CUDA(cudaFreeAsync(newLeaves, mStream));
         mStage.clear();
         mStageMaxN = 0;

@@ -62,6 +62,43 @@ void launchAssign(const KMeansLevel& lv, const NodeTile* tiles, const uint32_t* 
 // changed, activeCount = number of nodes updated.
 void launchUpdate(const KMeansLevel& lv, cudaStream_t s);
 
+// ------------------------------------------------------------------ float-center mode
+// fp32 centers (the FP64 quotient of the exact integer sums, rounded once), distances from the
+// tensor core in bf16 with each center split into hi + lo bf16 parts and fp32 accumulation, and
+// an FP64 re-score of every member whose best-versus-second margin is within the error bound.
+// Per node, `split` holds the MMA B operand: [2 K-blocks of 64 dims][32 rows][128 B] bf16 in the
+// 128-byte swizzled K-major layout, rows 0-15 the hi parts and rows 16-31 the lo parts.
+constexpr uint32_t kSplitBytes = 2 * 32 * 128;
+constexpr float kPadNormF = 3.0e38f; // |c|^2 of padding slots: never the argmin
+
+struct KMeansLevelF {
+    KMeansLevel base;             // members, groups, assign, counts, sums, change counters, err
+    float* centers;               // [nbNodes][16][128] this level's slice
+    uint8_t* split;               // [nbNodes][kSplitBytes]
+    float* cn;                    // [nbNodes][16] |c|^2 rounded to fp32 (kPadNormF for padding)
+    float2* bound;                // [nbNodes] (max |c|, max |c|^2) over the valid centers
+    unsigned long long* q;        // [nbNodes][16] sums of |x|^2 of each center's members
+    double* inertiaNode;          // [nbNodes] FP64 inertia of the node's last assignment
+    unsigned long long* refined;  // [2] members re-scored in FP64, members assigned (accumulated)
+    uint32_t lookupOnly;          // 1: assignment only (lookup through a float tree)
+};
+
+// fp32 centers from this level's uint8 initial centers (base.centers), then split, norms, bound.
+void launchCentersToFloat(const KMeansLevelF& lv, cudaStream_t s);
+// Split, norms and bound of nbNodes nodes of fp32 centers (tree upload / deserialisation).
+void launchPrepareFloatNodes(const float* centers, uint8_t* split, float* cn, float2* bound, uint64_t nbNodes,
+                             uint32_t B, cudaStream_t s);
+// One assign step (build) or one level of a lookup (lookupOnly) over 128-member node tiles.
+void launchAssignF(const KMeansLevelF& lv, const NodeTile* tiles, const uint32_t* nTilesDev, uint32_t maxTiles,
+                   cudaStream_t s);
+// One update step: inertia of the assignment just made, c = float(double(sum) / double(count)).
+void launchUpdateF(const KMeansLevelF& lv, cudaStream_t s);
+// out[0] = sum of inertiaNode[0, nbNodes) in a fixed order (deterministic).
+void launchInertiaSum(const double* inertiaNode, uint32_t nbNodes, double* out, cudaStream_t s);
+// Leaf of every member of the last level: leaf[members[i]] = node(i) * B + assign[i].
+void launchWriteLeaves(const KMeansLevel& lv, const NodeTile* tiles, const uint32_t* nTilesDev, uint32_t maxTiles,
+                       uint32_t* leaf, cudaStream_t s);
+
 // Stable regroup of every node's members by assignment (Vocabulary.cpp:83-98):
 // children (g, b) are laid out in order g*B + b; childCnt/childOff have nbNodes*B entries.
 struct RegroupScratch {

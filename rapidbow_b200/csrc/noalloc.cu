@@ -62,6 +62,8 @@ extern "C" int rbw_voc_lookup_noalloc(const rbw_vocabulary* voc, const void* dev
 {
     return rbw::runGuarded([&] {
         const rbw::Vocabulary& v = rbw::vocabularyOf(voc);
+        if (v.floatCenters())
+            throw rbw::Error(rbw::kUnsupported, "rbw_voc_lookup_noalloc: float-center vocabularies are not supported");
         const size_t need = rbw::lookupScratchBytes(v.branch(), v.levels(), nb_desc);
         if (need > rbw::kNoAllocScratchBytes) {
             throw rbw::Error(rbw::kInvalidArg,

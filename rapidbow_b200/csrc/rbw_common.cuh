@@ -242,6 +242,18 @@ __device__ __forceinline__ void mmaU8(uint32_t dTmem, uint64_t aDesc, uint64_t b
         "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
         : "memory");
 }
+// D[tmem] (+)= A[smem] * B[smem]^T, bf16 x bf16 -> fp32, M = 128, N from idesc.
+__device__ __forceinline__ void mmaBf16(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc,
+                                        uint32_t accumulate)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dTmem),
+        "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
 // Arrive (once) on `bar` when all previously issued MMAs of this thread have completed.
 __device__ __forceinline__ void mmaCommit(uint64_t* bar)
 {
@@ -293,6 +305,16 @@ __host__ __device__ constexpr uint32_t idescU8(uint32_t n)
     return (2u << 4)              // D = S32
            | (0u << 7)            // A = UINT8
            | (0u << 10)           // B = UINT8
+           | ((n >> 3) << 17)     // N
+           | ((128u >> 4) << 24); // M
+}
+
+// Instruction descriptor (M = 128, K-major A and B, bf16 x bf16 -> fp32).
+__host__ __device__ constexpr uint32_t idescBf16(uint32_t n)
+{
+    return (1u << 4)              // D = F32
+           | (1u << 7)            // A = BF16
+           | (1u << 10)           // B = BF16
            | ((n >> 3) << 17)     // N
            | ((128u >> 4) << 24); // M
 }

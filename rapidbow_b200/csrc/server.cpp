@@ -68,7 +68,7 @@ public:
     {
         if (mOpt.max_batch_queries == 0 || mOpt.max_batch_descriptors == 0 || mOpt.max_inflight_batches == 0)
             throw Error(kInvalidArg, "server limits must be positive");
-        if (mOpt.max_results == 0 || mOpt.max_results > 1024) throw Error(kUnsupported, "max_results must be 1..1024");
+        if (mOpt.max_results == 0) throw Error(kInvalidArg, "max_results must be positive");
         RBW_CUDA(cudaGetDevice(&mDevice));
         const Vocabulary& v = vocabularyOf(voc);
         mLevels = v.levels();
@@ -119,7 +119,6 @@ public:
     {
         if (n && desc == nullptr) throw Error(kInvalidArg, "null descriptors");
         if (n > mOpt.max_batch_descriptors) throw Error(kInvalidArg, "request larger than a batch");
-        if (n > 32768) throw Error(kUnsupported, "a query may hold at most 32768 descriptors");
         if (estimate(n, 1) > mOpt.hbm_budget_bytes) throw Error(kOutOfMemory, "request larger than the memory budget");
         auto r = std::make_shared<Request>();
         r->desc.assign(desc, desc + size_t(n) * 128);
@@ -209,17 +208,45 @@ private:
                       (1u << 20));
     }
 
+    // Device memory free right now: the driver's free memory plus what the library's pool holds
+    // unused (memory freed by finished batches stays in the pool for the next ones).
+    size_t liveFreeBytes() const
+    {
+        size_t freeB = 0, totalB = 0;
+        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) return 0;
+        cudaMemPool_t pool = libraryPool();
+        uint64_t reserved = 0, used = 0;
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+        return freeB + (reserved > used ? size_t(reserved - used) : 0);
+    }
+
+    // A batch of `bytes` is admitted while it fits what the batches in flight leave of the budget
+    // and the device memory free right now (less kLiveHeadroom).  With nothing in flight the
+    // live check is skipped, so memory held by other users cannot stall the queue; the batch
+    // then fails with RBW_ERR_OUT_OF_MEMORY if its allocations do.
+    static constexpr size_t kLiveHeadroom = size_t(256) << 20;
+    bool admits(size_t bytes, size_t liveFree) const
+    {
+        if (bytes + mReserved > mOpt.hbm_budget_bytes) return false;
+        if (mInflight.empty() && mReserved == 0) return true;
+        return bytes + kLiveHeadroom <= liveFree;
+    }
+
     void dispatchLoop()
     {
         cudaSetDevice(mDevice);
         for (;;) {
             std::unique_lock<std::mutex> lk(mMu);
             Slot* slot = nullptr;
+            size_t liveFree = 0;
             mCv.wait(lk, [&] {
                 if (mStop) return true;
                 if (mPending.empty()) return false;
                 slot = freeSlot();
-                return slot != nullptr && estimate(mPending.front()->n, 1) + mReserved <= mOpt.hbm_budget_bytes;
+                if (slot == nullptr) return false;
+                liveFree = liveFreeBytes();
+                return admits(estimate(mPending.front()->n, 1), liveFree);
             });
             if (mStop) {
                 for (auto& r : mPending) finishLocked(*r, RBW_ERR_INVALID_ARG, "server stopped");
@@ -234,7 +261,7 @@ private:
             while (!mPending.empty() && slot->reqs.size() < mOpt.max_batch_queries) {
                 const auto& r = mPending.front();
                 if (desc + r->n > mOpt.max_batch_descriptors) break;
-                if (estimate(desc + r->n, slot->reqs.size() + 1) + mReserved > mOpt.hbm_budget_bytes) break;
+                if (!slot->reqs.empty() && !admits(estimate(desc + r->n, slot->reqs.size() + 1), liveFree)) break;
                 desc += r->n;
                 slot->reqs.push_back(r);
                 mPending.pop_front();

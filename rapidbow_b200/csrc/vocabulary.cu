@@ -38,7 +38,8 @@ void DeviceBuffer::reset(size_t bytes)
 
 namespace {
 
-constexpr uint32_t kBlobExtMagic = 0x32574252u; // "RBW2": blobs with B != 16
+constexpr uint32_t kBlobExtMagic = 0x32574252u;   // "RBW2": blobs with B != 16
+constexpr uint32_t kBlobFloatMagic = 0x33574252u; // "RBW3": blobs with fp32 centers
 
 __global__ void swizzleKernel(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, uint64_t nbNodes)
 {
@@ -85,6 +86,24 @@ __global__ void padKernel(const uint8_t* __restrict__ canon, uint8_t* __restrict
     uint4 v = make_uint4(0, 0, 0, 0);
     if (b < B) v = reinterpret_cast<const uint4*>(canon + (node * B + b) * kDims)[chunk];
     reinterpret_cast<uint4*>(padded)[i] = v;
+}
+
+__global__ void padFloatKernel(const float* __restrict__ canon, float* __restrict__ padded, uint64_t nbNodes, uint32_t B)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; // (node, slot, dim)
+    if (i >= nbNodes * kMaxBranch * kDims) return;
+    const uint32_t d = i % kDims;
+    const uint32_t b = (i / kDims) % kMaxBranch;
+    const uint64_t node = i / (uint64_t(kDims) * kMaxBranch);
+    padded[i] = b < B ? canon[(node * B + b) * kDims + d] : 0.f;
+}
+
+__global__ void roundCentersKernel(const float* __restrict__ f, uint8_t* __restrict__ u, uint64_t count, uint32_t B)
+{
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint32_t b = (i / kDims) % kMaxBranch;
+    u[i] = b < B ? static_cast<uint8_t>(fminf(fmaxf(rintf(f[i]), 0.f), 255.f)) : uint8_t(0);
 }
 
 __global__ void iotaKernel(uint32_t* p, uint64_t n)
@@ -152,6 +171,69 @@ void Vocabulary::finalizeDevice(cudaStream_t stream)
     normsKernel<<<blocksFor(mNbNodes * kMaxBranch, 256), 256, 0, stream>>>(mCenters.as<uint8_t>(),
                                                                            mCnorm.as<int32_t>(), mNbNodes, mB);
     RBW_CUDA(cudaGetLastError());
+}
+
+void Vocabulary::allocateFloat()
+{
+    const uint64_t nodes = mNbNodes;
+    mCentersF.reset(nodes * kMaxBranch * kDims * sizeof(float));
+    mSplit.reset(nodes * kSplitBytes);
+    mCnF.reset(nodes * kMaxBranch * sizeof(float));
+    mBound.reset(nodes * sizeof(float2));
+    mRefined.reset(2 * sizeof(unsigned long long));
+    RBW_CUDA(cudaMemset(mRefined.get(), 0, 2 * sizeof(unsigned long long)));
+    mFloat = true;
+}
+
+void Vocabulary::roundFloatCenters(cudaStream_t stream)
+{
+    const uint64_t count = mNbNodes * kMaxBranch * kDims;
+    roundCentersKernel<<<blocksFor(count, 256), 256, 0, stream>>>(mCentersF.as<float>(), mCenters.as<uint8_t>(), count,
+                                                                  mB);
+    RBW_CUDA(cudaGetLastError());
+}
+
+std::unique_ptr<Vocabulary> Vocabulary::fromHostF32(uint32_t B, uint32_t L, const float* centers,
+                                                    const uint32_t* masks, const float* weights)
+{
+    std::unique_ptr<Vocabulary> v{new Vocabulary};
+    v->allocate(B, L);
+    v->allocateFloat();
+    const uint64_t nodes = v->mNbNodes;
+    DeviceBuffer canon(nodes * B * kDims * sizeof(float));
+    RBW_CUDA(cudaMemcpy(canon.get(), centers, canon.bytes(), cudaMemcpyHostToDevice));
+    padFloatKernel<<<blocksFor(nodes * kMaxBranch * kDims, 256), 256>>>(canon.as<float>(), v->mCentersF.as<float>(),
+                                                                        nodes, B);
+    RBW_CUDA(cudaGetLastError());
+    launchPrepareFloatNodes(v->mCentersF.as<float>(), v->mSplit.as<uint8_t>(), v->mCnF.as<float>(),
+                            v->mBound.as<float2>(), nodes, B, nullptr);
+    v->roundFloatCenters(nullptr);
+    v->mMasks.assign(masks, masks + nodes);
+    v->mWeights.assign(weights, weights + nodes * B);
+    v->finalizeDevice(nullptr);
+    RBW_CUDA(cudaDeviceSynchronize());
+    return v;
+}
+
+std::vector<float> Vocabulary::centersF32Host() const
+{
+    if (!mFloat) throw Error(kUnsupported, "the vocabulary has uint8 centers");
+    std::vector<float> padded(mNbNodes * kMaxBranch * kDims);
+    RBW_CUDA(cudaMemcpy(padded.data(), mCentersF.get(), padded.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    std::vector<float> out(mNbNodes * mB * kDims);
+    for (uint64_t n = 0; n < mNbNodes; n++)
+        std::memcpy(out.data() + n * mB * kDims, padded.data() + n * kMaxBranch * kDims,
+                    size_t(mB) * kDims * sizeof(float));
+    return out;
+}
+
+uint64_t Vocabulary::takeRefinedLookups() const
+{
+    if (!mFloat) return 0;
+    unsigned long long v[2] = {0, 0};
+    RBW_CUDA(cudaMemcpy(v, mRefined.get(), sizeof(v), cudaMemcpyDeviceToHost));
+    RBW_CUDA(cudaMemset(mRefined.get(), 0, sizeof(v)));
+    return v[0];
 }
 
 std::unique_ptr<Vocabulary> Vocabulary::fromHost(uint32_t B, uint32_t L, const uint8_t* centers, const uint32_t* masks,
@@ -222,6 +304,10 @@ uint32_t Vocabulary::lookup(const uint8_t* devDesc, uint64_t n, uint32_t* devLea
     if (devDesc == nullptr || devLeaf == nullptr) throw Error(kInvalidArg, "null buffer");
     if (reinterpret_cast<uintptr_t>(devDesc) % 16 != 0)
         throw Error(kInvalidArg, "descriptors must be 16-byte aligned");
+    if (mFloat) {
+        if (algo == kLookupSimtF32) throw Error(kUnsupported, "the FP32 SIMT lookup reads uint8 centers");
+        return lookupFloat(devDesc, n, devLeaf, stream);
+    }
     if (algo == kLookupAuto) algo = kLookupTensorU8;
     LookupScratch s{};
     if (algo == kLookupSimtF32) {
@@ -352,6 +438,8 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
     const uint32_t check = std::max(1u, opts.checkInterval);
     std::unique_ptr<Vocabulary> voc{new Vocabulary};
     voc->allocate(B, L);
+    const bool fl = opts.floatCenters;
+    if (fl) voc->allocateFloat();
     RBW_CUDA(cudaMemsetAsync(voc->mCenters.get(), 0, voc->mCenters.bytes(), stream));
     const uint64_t n = nbDesc;
     const uint64_t maxLevelNodes = ipow(B, L - 1);
@@ -372,6 +460,16 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
     StreamBuffer tileHist(uint64_t(B) * maxTiles32 * 4, st), tileScan(uint64_t(B) * maxTiles32 * 4, st);
     uint32_t* totals = small.as<uint32_t>();
     uint32_t* activeCount = small.as<uint32_t>() + 4;
+    // float centers: member |x|^2 sums, per-node inertia, the level's inertia per step, counters
+    StreamBuffer qSums(fl ? maxLevelNodes * kMaxBranch * 8 : 0, st), inertiaNode(fl ? maxLevelNodes * 8 : 0, st);
+    StreamBuffer inertiaTrace(fl ? uint64_t(opts.maxIterations) * 8 : 0, st), counters(fl ? uint64_t(L) * 16 : 0, st);
+    if (fl) {
+        RBW_CUDA(cudaMemsetAsync(qSums.get(), 0, qSums.bytes(), stream));
+        RBW_CUDA(cudaMemsetAsync(inertiaNode.get(), 0, inertiaNode.bytes(), stream));
+        RBW_CUDA(cudaMemsetAsync(counters.get(), 0, counters.bytes(), stream));
+    }
+    std::vector<double> hostFirst(L, 0.0), hostLast(L, 0.0);
+    std::vector<unsigned long long> hostCounters(2 * size_t(L), 0ull);
 
     iotaKernel<<<blocksFor(n, 256), 256, 0, stream>>>(members.as<uint32_t>(), n);
     RBW_CUDA(cudaGetLastError());
@@ -386,7 +484,7 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
     voc->mMasks.assign(voc->mNbNodes, 0u);
     std::mt19937_64 rng{}; // kmeans.cpp:145 (default seed)
     std::vector<uint32_t> hostCnt, hostPicks, hostNValid;
-    if (stats) *stats = BuildStats{};
+    BuildStats bs{};
 
     for (uint32_t level = 0; level < L; level++) {
         const uint32_t nbLv = static_cast<uint32_t>(ipow(B, level));
@@ -409,6 +507,18 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
         lv.activeCount = activeCount;
         lv.ieeeDivision = opts.ieeeDivision ? 1u : 0u;
         lv.err = voc->mErrors.as<DeviceErrors>();
+        KMeansLevelF lvf{};
+        if (fl) {
+            lvf.base = lv;
+            lvf.centers = voc->mCentersF.as<float>() + lb * kMaxBranch * kDims;
+            lvf.split = voc->mSplit.as<uint8_t>() + lb * kSplitBytes;
+            lvf.cn = voc->mCnF.as<float>() + lb * kMaxBranch;
+            lvf.bound = voc->mBound.as<float2>() + lb;
+            lvf.q = qSums.as<unsigned long long>();
+            lvf.inertiaNode = inertiaNode.as<double>();
+            lvf.refined = counters.as<unsigned long long>() + 2 * level;
+            lvf.lookupOnly = 0;
+        }
 
         // ---- initial centers
         if (opts.initMode == kInitReference) {
@@ -448,7 +558,11 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
             launchInitCentersFromDesc(lv, picks.as<uint32_t>(), n, stream);
             RBW_CUDA(cudaStreamSynchronize(stream));
         }
-        launchCenterNorms(lv, stream);
+        if (fl) {
+            launchCentersToFloat(lvf, stream);
+        } else {
+            launchCenterNorms(lv, stream);
+        }
 
         // ---- Lloyd iterations (kmeans.cpp:118-133)
         buildNodeTiles(lv.nodeCnt, lv.nodeOff, nbLv, 128, tileOff.as<uint32_t>(), scanTmp.as<uint32_t>(),
@@ -457,9 +571,16 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
         RBW_CUDA(cudaMemsetAsync(lastChanged.get(), 0xFF, uint64_t(nbLv) * 4, stream));
         uint32_t iters = 0;
         for (uint32_t it = 0; it < opts.maxIterations; it++) {
-            launchAssign(lv, tiles128.as<NodeTile>(), totals, maxTiles128, stream);
-            RBW_CUDA(cudaMemsetAsync(activeCount, 0, 4, stream));
-            launchUpdate(lv, stream);
+            if (fl) {
+                launchAssignF(lvf, tiles128.as<NodeTile>(), totals, maxTiles128, stream);
+                RBW_CUDA(cudaMemsetAsync(activeCount, 0, 4, stream));
+                launchUpdateF(lvf, stream);
+                launchInertiaSum(inertiaNode.as<double>(), nbLv, inertiaTrace.as<double>() + it, stream);
+            } else {
+                launchAssign(lv, tiles128.as<NodeTile>(), totals, maxTiles128, stream);
+                RBW_CUDA(cudaMemsetAsync(activeCount, 0, 4, stream));
+                launchUpdate(lv, stream);
+            }
             iters = it + 1;
             if ((it + 1) % check == 0 || it + 1 == opts.maxIterations) {
                 uint32_t active = 0;
@@ -468,7 +589,12 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
                 if (active == 0) break;
             }
         }
-        if (stats && level < 16) stats->iterations[level] = iters;
+        if (level < 16) bs.iterations[level] = iters;
+        if (fl) {
+            RBW_CUDA(cudaMemcpyAsync(&hostFirst[level], inertiaTrace.get(), 8, cudaMemcpyDeviceToHost, stream));
+            RBW_CUDA(cudaMemcpyAsync(&hostLast[level], inertiaTrace.as<double>() + (iters - 1), 8,
+                                     cudaMemcpyDeviceToHost, stream));
+        }
 
         // ---- stable regroup into the next level's nodes (Vocabulary.cpp:83-98)
         RegroupScratch rs{tileHist.as<uint32_t>(), tileScan.as<uint32_t>(), scanTmp.as<uint32_t>(),
@@ -480,26 +606,118 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
         std::swap(nodeCnt, childCnt);
         std::swap(nodeOff, childOff);
     }
+    if (fl) {
+        RBW_CUDA(cudaMemcpyAsync(hostCounters.data(), counters.get(), hostCounters.size() * 8, cudaMemcpyDeviceToHost,
+                                 stream));
+    }
     RBW_CUDA(cudaStreamSynchronize(stream));
     voc->mWeights.resize(voc->mNbNodes * B);
     for (size_t i = 0; i < occ.size(); i++) voc->mWeights[i] = idfWeight(nbDoc, occ[i]);
+    if (fl) voc->roundFloatCenters(stream);
     voc->finalizeDevice(stream);
     RBW_CUDA(cudaStreamSynchronize(stream));
     const DeviceErrors e = voc->takeDeviceErrors();
     if (e.code != 0)
         throw Error(kTimeout, "a bounded device wait gave up during the build (site " + std::to_string(e.where) + ")");
-    if (stats) {
-        stats->levels = L;
-        stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
+    bs.levels = L;
+    for (uint32_t level = 0; level < L && level < 16; level++) {
+        bs.inertiaFirst[level] = hostFirst[level];
+        bs.inertiaLast[level] = hostLast[level];
+        bs.refined[level] = hostCounters[2 * level];
+        bs.assignments[level] = hostCounters[2 * level + 1];
     }
+    bs.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
+    voc->mStats = bs;
+    if (stats) *stats = bs;
     return voc;
+}
+
+uint32_t Vocabulary::lookupFloat(const uint8_t* devDesc, uint64_t nTotal, uint32_t* devLeaf, cudaStream_t stream) const
+{
+    // Level by level: the descriptors grouped by node, one split-bf16 assign launch over all the
+    // level's nodes (FP64 re-score near ties), then the stable regroup into the children.
+    const uint32_t B = mB, L = mL;
+    const uint64_t chunk = std::min<uint64_t>(nTotal, 1ull << 27);
+    const uint64_t maxLevelNodes = ipow(B, L - 1);
+    const uint32_t maxTiles128 = static_cast<uint32_t>(chunk / 128 + maxLevelNodes + 1);
+    const uint32_t maxTiles32 = static_cast<uint32_t>(chunk / 32 + maxLevelNodes + 1);
+    const cudaStream_t st = stream;
+    StreamBuffer members(chunk * 4, st), members2(chunk * 4, st), assign(chunk, st);
+    StreamBuffer nodeCnt(maxLevelNodes * 4, st), nodeOff(maxLevelNodes * 4, st);
+    StreamBuffer childCnt(maxLevelNodes * 4, st), childOff(maxLevelNodes * 4, st), small(64, st);
+    StreamBuffer tiles128(uint64_t(maxTiles128) * sizeof(NodeTile), st);
+    StreamBuffer tiles32(uint64_t(maxTiles32) * sizeof(NodeTile), st), tileOff(maxLevelNodes * 4, st);
+    StreamBuffer scanTmp(scanTempWords(std::max<uint64_t>(uint64_t(B) * maxTiles32, maxLevelNodes)) * 4, st);
+    StreamBuffer tileHist(uint64_t(B) * maxTiles32 * 4, st), tileScan(uint64_t(B) * maxTiles32 * 4, st);
+    uint32_t* totals = small.as<uint32_t>();
+    uint32_t kernels = 0;
+    for (uint64_t off = 0; off < nTotal; off += chunk) {
+        const uint32_t n = static_cast<uint32_t>(std::min(chunk, nTotal - off));
+        iotaKernel<<<blocksFor(n, 256), 256, 0, stream>>>(members.as<uint32_t>(), n);
+        RBW_CUDA(cudaGetLastError());
+        const uint32_t zero = 0;
+        RBW_CUDA(cudaMemcpyAsync(nodeCnt.get(), &n, 4, cudaMemcpyHostToDevice, stream));
+        RBW_CUDA(cudaMemcpyAsync(nodeOff.get(), &zero, 4, cudaMemcpyHostToDevice, stream));
+        kernels++;
+        for (uint32_t level = 0; level < L; level++) {
+            const uint32_t nbLv = static_cast<uint32_t>(ipow(B, level));
+            const uint64_t lb = levelBeg(B, level);
+            KMeansLevel lv{};
+            lv.B = B;
+            lv.nbNodes = nbLv;
+            lv.nbMembers = n;
+            lv.desc = devDesc + off * kDims;
+            lv.members = members.as<uint32_t>();
+            lv.nodeOff = nodeOff.as<uint32_t>();
+            lv.nodeCnt = nodeCnt.as<uint32_t>();
+            lv.assign = assign.as<uint8_t>();
+            lv.err = mErrors.as<DeviceErrors>();
+            KMeansLevelF lvf{};
+            lvf.base = lv;
+            lvf.centers = mCentersF.as<float>() + lb * kMaxBranch * kDims;
+            lvf.split = mSplit.as<uint8_t>() + lb * kSplitBytes;
+            lvf.cn = mCnF.as<float>() + lb * kMaxBranch;
+            lvf.bound = mBound.as<float2>() + lb;
+            lvf.refined = mRefined.as<unsigned long long>();
+            lvf.lookupOnly = 1;
+            buildNodeTiles(lv.nodeCnt, lv.nodeOff, nbLv, 128, tileOff.as<uint32_t>(), scanTmp.as<uint32_t>(),
+                           tiles128.as<NodeTile>(), maxTiles128, totals, stream);
+            launchAssignF(lvf, tiles128.as<NodeTile>(), totals, maxTiles128, stream);
+            kernels += 7;
+            if (level + 1 == L) {
+                launchWriteLeaves(lv, tiles128.as<NodeTile>(), totals, maxTiles128, devLeaf + off, stream);
+                kernels++;
+            } else {
+                RegroupScratch rs{tileHist.as<uint32_t>(), tileScan.as<uint32_t>(), scanTmp.as<uint32_t>(),
+                                  tiles32.as<NodeTile>(), tileOff.as<uint32_t>(), totals, maxTiles32};
+                launchRegroup(lv, rs, members2.as<uint32_t>(), childCnt.as<uint32_t>(), childOff.as<uint32_t>(),
+                              stream);
+                kernels += 11;
+                std::swap(members, members2);
+                std::swap(nodeCnt, childCnt);
+                std::swap(nodeOff, childOff);
+            }
+        }
+    }
+    return kernels;
 }
 
 std::vector<uint8_t> Vocabulary::serialize() const
 {
-    const std::vector<uint8_t> c = centersHost();
     const uint64_t nodes = mNbNodes;
     std::vector<uint8_t> out;
+    if (mFloat) {
+        // [u32 magic][u32 B][u32 L][f32 centers nodes x B x 128][u32 mask x nodes][f32[B] x nodes]
+        const std::vector<float> cf = centersF32Host();
+        out.resize(12 + cf.size() * 4 + nodes * 4 + nodes * mB * 4);
+        const uint32_t hdr[3] = {kBlobFloatMagic, mB, mL};
+        std::memcpy(out.data(), hdr, 12);
+        std::memcpy(out.data() + 12, cf.data(), cf.size() * 4);
+        std::memcpy(out.data() + 12 + cf.size() * 4, mMasks.data(), nodes * 4);
+        std::memcpy(out.data() + 12 + cf.size() * 4 + nodes * 4, mWeights.data(), nodes * mB * 4);
+        return out;
+    }
+    const std::vector<uint8_t> c = centersHost();
     if (mB == 16) {
         // [u32 L][Node: uint32[32 words][16 centers] x nodes][u16 mask x nodes][float[16] x nodes]
         out.resize(4 + nodes * (2048 + 2 + 64));
@@ -532,6 +750,23 @@ std::unique_ptr<Vocabulary> Vocabulary::deserialize(const uint8_t* blob, size_t 
     if (blob == nullptr || size < 4) throw Error(kInvalidBlob, "invalid blob");
     uint32_t first = 0;
     std::memcpy(&first, blob, 4);
+    if (first == kBlobFloatMagic) {
+        if (size < 12) throw Error(kInvalidBlob, "invalid blob");
+        uint32_t B = 0, L = 0;
+        std::memcpy(&B, blob + 4, 4);
+        std::memcpy(&L, blob + 8, 4);
+        if (B < 2 || B > 16 || L < 1 || L > 8) throw Error(kInvalidBlob, "invalid blob");
+        const uint64_t nodes = levelBeg(B, L);
+        const uint64_t cBytes = nodes * B * kDims * 4;
+        if (size != 12 + cBytes + nodes * 4 + nodes * B * 4) throw Error(kInvalidBlob, "invalid blob");
+        std::vector<float> centers(nodes * B * kDims);
+        std::vector<uint32_t> masks(nodes);
+        std::vector<float> weights(nodes * B);
+        std::memcpy(centers.data(), blob + 12, cBytes);
+        std::memcpy(masks.data(), blob + 12 + cBytes, nodes * 4);
+        std::memcpy(weights.data(), blob + 12 + cBytes + nodes * 4, nodes * B * 4);
+        return fromHostF32(B, L, centers.data(), masks.data(), weights.data());
+    }
     if (first == kBlobExtMagic) {
         if (size < 12) throw Error(kInvalidBlob, "invalid blob");
         uint32_t B = 0, L = 0;

@@ -48,11 +48,16 @@ struct BuildOptions {
     uint64_t seed = 0;
     const uint32_t* injected = nullptr; // host [levelBeg(L)][B] descriptor indices
     bool ieeeDivision = false;          // center update rounding: false = reference (fast-math)
+    bool floatCenters = false;          // fp32 centers, split-bf16 distances with FP64 re-score
 };
 
 struct BuildStats {
     uint32_t levels = 0;
     uint32_t iterations[16] = {};     // Lloyd steps run per level
+    double inertiaFirst[16] = {};     // float centers: FP64 inertia after the level's first step
+    double inertiaLast[16] = {};      //                and after its last step
+    uint64_t refined[16] = {};        // float centers: assignments re-scored in FP64, all steps
+    uint64_t assignments[16] = {};    //                assignments made, all steps
     double seconds = 0;
 };
 
@@ -63,6 +68,10 @@ public:
     // masks [levelBeg(L)] (bit b = valid center), weights [levelBeg(L)][B].
     static std::unique_ptr<Vocabulary> fromHost(uint32_t B, uint32_t L, const uint8_t* centers, const uint32_t* masks,
                                                 const float* weights);
+    // The same with fp32 centers [levelBeg(L)][B][128]: lookups descend with split-bf16
+    // distances and an FP64 re-score near ties.
+    static std::unique_ptr<Vocabulary> fromHostF32(uint32_t B, uint32_t L, const float* centers,
+                                                   const uint32_t* masks, const float* weights);
     // Hierarchical k-means build on the GPU (Vocabulary.cpp:32-121).  Synchronous.
     static std::unique_ptr<Vocabulary> build(uint32_t B, uint32_t L, const uint8_t* devDesc, uint32_t nbDesc,
                                              uint32_t nbDoc, const BuildOptions& opts, cudaStream_t stream,
@@ -77,9 +86,15 @@ public:
     const float* levelWeights(uint32_t level) const; // host, [levelSize(level)][B]
     const std::vector<float>& weights() const { return mWeights; }
     const std::vector<uint32_t>& masks() const { return mMasks; }
-    // Canonical host copy of the centers ([nbNodes][B][128]).
+    // Canonical host copy of the centers ([nbNodes][B][128]); fp32 centers rounded to uint8.
     std::vector<uint8_t> centersHost() const;
+    bool floatCenters() const { return mFloat; }
+    // fp32 centers ([nbNodes][B][128]) of a float-center vocabulary.
+    std::vector<float> centersF32Host() const;
     const DeviceTree& deviceTree() const { return mTree; }
+    const BuildStats& buildStats() const { return mStats; }
+    // Reads and clears the count of lookup descriptors re-scored in FP64 (float centers).
+    uint64_t takeRefinedLookups() const;
 
     // Stream-ordered lookup; scratch comes from the stream-ordered allocator (or `scratch` if
     // non-null, `scratchBytes` >= lookupScratchBytes).  Returns kernels launched.
@@ -91,7 +106,10 @@ public:
 private:
     Vocabulary() = default;
     void allocate(uint32_t B, uint32_t L);
+    void allocateFloat();
     void finalizeDevice(cudaStream_t stream); // swizzled copy + norms from mCenters
+    void roundFloatCenters(cudaStream_t stream); // mCenters = uint8 rounding of mCentersF
+    uint32_t lookupFloat(const uint8_t* devDesc, uint64_t n, uint32_t* devLeaf, cudaStream_t stream) const;
 
     uint32_t mB = 0;
     uint32_t mL = 0;
@@ -103,6 +121,14 @@ private:
     std::vector<uint32_t> mMasks;
     std::vector<float> mWeights;
     DeviceTree mTree;
+    // float-center vocabularies
+    bool mFloat = false;
+    DeviceBuffer mCentersF;  // [nbNodes][16][128] float
+    DeviceBuffer mSplit;     // [nbNodes][kSplitBytes] bf16 hi/lo MMA operand
+    DeviceBuffer mCnF;       // [nbNodes][16] float |c|^2
+    DeviceBuffer mBound;     // [nbNodes] float2
+    DeviceBuffer mRefined;   // u64: lookup descriptors re-scored in FP64
+    BuildStats mStats;
 };
 
 // Library-owned stream-ordered memory pool: freed blocks stay cached for the next call.

@@ -226,6 +226,47 @@ def test_many_documents_use_global_accumulators(oracle):
         odb.add(int(i), d)
     for q in make_queries(docs, B ** L, 8, seed=1):
         check_query(db, odb, q, 50)
+    # k above the shared-memory selection (1024): shard candidates and the merge in global memory
+    for q in make_queries(docs, B ** L, 3, seed=2):
+        check_query(db, odb, np.concatenate([q, np.arange(0, B ** L, 7, dtype=np.uint32)]), 1500)
+
+
+def test_large_documents_queries_and_result_sets(oracle):
+    """Documents and queries above 32,768 descriptors (sorted in global memory) and k = 2,000
+    (selected in global memory) against the oracle, single and batched; the reference's
+    DataBase takes any size (DataBase.cpp:39-69,71-190)."""
+    import torch
+
+    B, L = 16, 3
+    n_leaves = B ** L
+    rng = np.random.default_rng(62)
+    docs = make_docs(2600, n_leaves, seed=61, lo=20, hi=300)
+    big = [rng.integers(0, n_leaves, 40000, dtype=np.uint32), rng.integers(0, n_leaves, 70001, dtype=np.uint32)]
+    big[0][:5000] = docs[7][0]  # a long run of one leaf (tf = 5000+)
+    docs = docs + big
+    ids = np.arange(len(docs), dtype=np.uint32)
+    _, db, odb, _ = build_pair(oracle, B, L, docs, ids)
+    for i in (len(docs) - 2, len(docs) - 1):
+        assert np.float32(db.doc_rcp(int(i))) == np.float32(odb.doc_rcp(int(i)))
+    leaf = int(docs[7][0])
+    assert np.array_equal(db.postings(leaf), odb.postings(leaf))
+    qs = [np.concatenate([docs[-1][:30000], rng.integers(0, n_leaves, 15000, dtype=np.uint32)]),
+          docs[5], rng.integers(0, n_leaves, 40000, dtype=np.uint32), docs[-2]]
+    for q in qs:
+        for k in (2000, 50):
+            check_query(db, odb, q, k)
+    k = 2000
+    offs = np.zeros(len(qs) + 1, np.int64)
+    offs[1:] = np.cumsum([q.size for q in qs])
+    leaves = torch.from_numpy(np.concatenate(qs).astype(np.int32)).cuda()
+    bd, bs, bc = db.query_batched(leaves, torch.from_numpy(offs).cuda(), k)
+    torch.cuda.synchronize()
+    bd, bs, bc = bd.cpu().numpy().view(np.uint32), bs.cpu().numpy(), bc.cpu().numpy()
+    for i, q in enumerate(qs):
+        d, s = db.query(q, k, with_scores=True)
+        assert bc[i] == d.size == min(k, len(docs))
+        assert np.array_equal(bd[i, : d.size], d)
+        assert np.array_equal(bs[i, : d.size], s)
 
 
 def test_edge_cases(oracle):
@@ -260,8 +301,8 @@ def test_edge_cases(oracle):
     # adding after a query rebuilds the index
     db.add_doc(11, np.array([9, 9], np.uint32))
     assert 11 in db.query(np.array([9, 9], np.uint32), 10).tolist()
-    with pytest.raises(rbw.RbwError):
-        db.query(np.array([5], np.uint32), 2000)
+    # max_results beyond every touched document: all of them (no limit on k)
+    assert np.array_equal(db.query(np.array([9, 5], np.uint32), 5000), got)
 
 
 def test_incremental_segments_match_oracle(oracle):

@@ -124,8 +124,16 @@ def test_overlap_and_errors(setup):
     assert st["mean_batch_requests"] <= 4
     with pytest.raises(rbw.RbwError):
         srv.wait(ids[0])                          # already collected
-    with pytest.raises(rbw.RbwError):
-        srv.submit(np.zeros((40000, 128), np.uint8))  # above 32768 descriptors
+    srv.close()
+    # a request above 32,768 descriptors is served like any other (sorted in global memory)
+    srv = rbw.Server(voc, db, max_results=5, max_batch_descriptors=60000)
+    big = np.concatenate([queries[0]] * (40000 // queries[0].shape[0] + 1))[:40000]
+    d, s, _ = srv.wait(srv.submit(big))
+    dd, ds = direct(voc, db, big, 5)
+    assert np.array_equal(d, dd) and np.array_equal(s, ds)
+    with pytest.raises(rbw.RbwError) as e:
+        srv.submit(np.zeros((60001, 128), np.uint8))  # larger than a batch
+    assert e.value.status == rbw.RBW_ERR_INVALID_ARG
     srv.close()
 
 
