@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--no-serving", action="store_true",
                    help="skip the serving workload (1M-word tree, 100,000 images, Poisson arrivals)")
     p.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own GPU lookup kernel")
+    p.add_argument("--no-tune", action="store_true", help="skip autotuning (built-in launch parameters)")
     p.add_argument("--serving-docs", type=int, default=100_000)
     p.add_argument("--serving-rate", type=float, default=2000.0, help="arrivals per second")
     p.add_argument("--serving-seconds", type=float, default=5.0)
@@ -267,6 +268,14 @@ def run_ours(args, world, rank, local):
             kern = rbw.timing_read(kernel_name)
         return allreduce_max(world, ms), launches, kern
 
+    # autotuning (before the timed region): rows per thread of the regroup scatter, on this lookup
+    tuned = None
+    if not args.no_tune:
+        from rapidbow_b200.autotune import Autotuner
+
+        e = Autotuner.for_current_device().tune_lookup(voc, desc)
+        tuned = {"param": "scatter_rows", "value": e["value"], "default": 16, "tuned_ms": e["ms"],
+                 "default_ms": e["default_ms"], "kernel": "scanBins + buildTiles + scatterRows (per lookup)"}
     with ClockSampler(local) as clocks:
         ms, launches, (k_ms, k_n) = timed("tensor_u8", args.steps, args.warmup, "lookup_pass_tc")
     clk = clocks.summary()
@@ -302,6 +311,8 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
         "device_errors": [code, where],
     }
+    if tuned is not None:
+        line["autotune"] = tuned
 
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         line["ref_gpu_kernel"] = ref_gpu_lookup(voc, desc, out, value)
@@ -568,16 +579,77 @@ def build_bench(args, dev, rank):
     del c0
     torch.cuda.empty_cache()
     c2 = sift_like(10_000_000, seed=2, n_components=4096, zipf=1.1, device=dev)
-    _, s2 = timed_build(c2, 10, 6, 3)
-    out["b10_l6_10m"] = {
-        "workload": "build: 10M SIFT-like descriptors (4,096-component mixture, Zipf(1.1) weights), B=10, L=6 "
-                    "(1M words), k-means++ init, 10 Lloyd iterations",
-        "value": s2, "unit": "s", "higher_is_better": False,
-        "note": "the reference supports B=16 only and cannot run this configuration",
-    }
+    wl2 = ("10M SIFT-like descriptors (4,096-component mixture, Zipf(1.1) weights), B=10, L=6 (1M words), "
+           "k-means++ init, 10 Lloyd iterations")
+    for key, fl in (("b10_l6_10m", False), ("b10_l6_10m_float", True)):
+        tune = None
+        if not args.no_tune:
+            from rapidbow_b200.autotune import Autotuner
+
+            e = Autotuner.for_current_device().tune_build(c2, 10, 6, float_centers=fl, repeats=1, nb_doc=1000,
+                                                          init="kmeans++", seed=7, max_iterations=10)
+            tune = {"param": e["param"], "value": e["value"], "tuned_assign_ms": e["ms"],
+                    "default_assign_ms": e["default_ms"]}
+        rbw.timing_reset()
+        rbw.timing_enable(True)
+        voc2, s2 = timed_build(c2, 10, 6, 3, float_centers=fl)
+        rbw.timing_enable(False)
+        a_ms, _ = rbw.timing_read("kmeans_assign")
+        u_ms, _ = rbw.timing_read("kmeans_update")
+        res = {"workload": ("build (float centers: split-bf16 distances, FP64 re-score, FP64 inertia): " if fl
+                            else "build (uint8 centers): ") + wl2,
+               "value": s2, "unit": "s", "higher_is_better": False,
+               "assign_kernel_ms_per_build": a_ms / 4, "update_kernel_ms_per_build": u_ms / 4,
+               "note": "the reference supports B=16 only and cannot run this configuration"}
+        if fl:
+            st = voc2.build_stats()
+            res["refined_descriptors"] = int(sum(st["refined"]))
+            res["assignments"] = int(sum(st["assignments"]))
+            res["inertia_first_last_by_level"] = [[a, b] for a, b in zip(st["inertia_first"], st["inertia_last"])]
+        if tune:
+            res["autotune"] = tune
+        out[key] = res
+        del voc2
     del c2
     torch.cuda.empty_cache()
+    if rank == 0 and not args.no_cpu_baseline:
+        out["b10_l4_1m_float_vs_fp64_oracle"] = float_build_check(dev)
     return out
+
+
+def float_build_check(dev):
+    """The float-center build against the FP64 oracle on 1M descriptors of the same generator
+    (B=10, L=4, k-means++ init, 10 Lloyd iterations): maximum relative center error, identical
+    occurrence counts (assignments), refined descriptors, and the oracle's time on all host
+    threads."""
+    import numpy as np
+    import torch
+
+    import rapidbow_b200 as rbw
+    from oracle.pyoracle import INIT_KMEANSPP, Oracle
+    from rapidbow_b200.synth import sift_like
+
+    d = sift_like(1_000_000, seed=12, n_components=4096, zipf=1.1, device=dev)
+    voc = rbw.build_vocabulary(d, 10, nb_doc=1000, nb_levels=4, init="kmeans++", seed=7, max_iterations=10,
+                               float_centers=True)
+    host = d.cpu().numpy()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ref = Oracle().build_vocabulary_f32(host, 1000, 10, 4, max_iter=10, init=INIT_KMEANSPP, seed=7, threads=threads)
+    cpu_s = time.perf_counter() - t0
+    got = voc.centers_f32().astype(np.float64)
+    want = ref["centers"].astype(np.float64)
+    rel = float(np.max(np.abs(got - want) / np.maximum(np.abs(want), 1e-30)))
+    st = voc.build_stats()
+    leaves = voc.lookup(d).cpu().numpy().view(np.uint32)
+    return {"workload": "1M descriptors of the 4,096-component Zipf(1.1) generator, B=10, L=4, k-means++, 10 iterations",
+            "max_relative_center_error": rel, "centers_bit_identical": bool(np.array_equal(got, want)),
+            "identical_occurrences": bool(np.array_equal(voc.tree()[2], ref["weights"])),
+            "word_ids_equal_fp64_lookup": bool(np.array_equal(leaves, Oracle().lookup_f32(ref["centers"], 10, 4, host,
+                                                                                          threads=threads))),
+            "refined_descriptors": int(sum(st["refined"])), "assignments": int(sum(st["assignments"])),
+            "cpu_baseline": {"value": cpu_s, "unit": "s", "cores": threads, "kind": "port",
+                             "sample": "the same build (FP64 oracle)"}}
 
 
 SERVING_WORKLOAD = ("serving: 1M-word tree (B=10, L=6) trained on 10M SIFT-like descriptors from a 4,096-component "

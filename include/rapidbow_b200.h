@@ -301,6 +301,24 @@ RBW_API int rbw_server_batch_bytes(rbw_server* server, uint64_t n_desc, uint32_t
 /* Fails requests still waiting, finishes the batches in flight. */
 RBW_API void rbw_server_destroy(rbw_server* server);
 
+/* ------------------------------------------------------------------ tuning
+ * No counterpart in the reference (which sizes its assign grid by an occupancy query,
+ * kmeans.cu:307-322).  Launch parameters picked by an autotuner (rapidbow_b200.autotune, which
+ * times the candidates on the caller's workload and keeps a per-device cache file), stored per
+ * (parameter, branch factor, tree levels, descriptor-count bucket = floor(log2(n))); levels 0
+ * matches any depth.  Unset entries use the defaults. */
+enum {
+    RBW_TUNE_ASSIGN_CTAS_PER_SM = 0,     /* uint8 k-means assign: CTAs per SM, 1..6 (default 6) */
+    RBW_TUNE_ASSIGN_F32_CTAS_PER_SM = 1, /* float-center assign: CTAs per SM, 1..3 (default 3) */
+    RBW_TUNE_SCATTER_ROWS = 2            /* lookup regroup: rows per thread, 8, 16 or 32 (default 16) */
+};
+/* value 0 removes the entry; RBW_ERR_INVALID_ARG for a value the parameter cannot take. */
+RBW_API int rbw_tuning_set(uint32_t param, uint32_t branch_factor, uint32_t nb_levels, uint32_t bucket,
+                           uint32_t value);
+/* The value a launch for n descriptors would use. */
+RBW_API int rbw_tuning_get(uint32_t param, uint32_t branch_factor, uint32_t nb_levels, uint64_t n, uint32_t* value);
+RBW_API int rbw_tuning_clear(void);
+
 /* Optional CUDA-event timing of this library's own kernel launches (no reference
  * counterpart; used by bench.py).  While enabled, each launch of a timed kernel is bracketed by
  * two events on its stream.  rbw_timing_read sums completed launches of one kernel id:

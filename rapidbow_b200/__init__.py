@@ -99,6 +99,9 @@ def load_library() -> C.CDLL:
         "rbw_voc_get_centers_f32": (C.c_int, [vp, vp]),
         "rbw_voc_build_stats": (C.c_int, [vp, C.POINTER(BuildStats)]),
         "rbw_voc_refined_lookups": (C.c_int, [vp, C.POINTER(u64)]),
+        "rbw_tuning_set": (C.c_int, [u32, u32, u32, u32, u32]),
+        "rbw_tuning_get": (C.c_int, [u32, u32, u32, u64, C.POINTER(u32)]),
+        "rbw_tuning_clear": (C.c_int, []),
         "rbw_timing_enable": (None, [i32]),
         "rbw_timing_reset": (C.c_int, []),
         "rbw_timing_read": (C.c_int, [u32, C.POINTER(C.c_double), C.POINTER(u64)]),

@@ -3,6 +3,7 @@
 #include "rapidbow_b200.h"
 #include "vocabulary.h"
 #include "timing.h"
+#include "tuning.h"
 #include "capi_internal.h"
 
 #include <cstring>
@@ -264,6 +265,28 @@ int rbw_voc_device_errors(const rbw_vocabulary* voc, uint32_t* code, uint32_t* w
 }
 
 void rbw_voc_destroy(rbw_vocabulary* voc) { delete voc; }
+
+int rbw_tuning_set(uint32_t param, uint32_t branch_factor, uint32_t nb_levels, uint32_t bucket, uint32_t value)
+{
+    return guard([&] {
+        if (param >= rbw::kTuneParamCount) throw rbw::Error(rbw::kInvalidArg, "unknown tuning parameter");
+        rbw::setTunedValue(static_cast<rbw::TuneParam>(param), branch_factor, nb_levels, bucket, value);
+    });
+}
+
+int rbw_tuning_get(uint32_t param, uint32_t branch_factor, uint32_t nb_levels, uint64_t n, uint32_t* value)
+{
+    return guard([&] {
+        if (param >= rbw::kTuneParamCount) throw rbw::Error(rbw::kInvalidArg, "unknown tuning parameter");
+        if (value == nullptr) throw rbw::Error(rbw::kInvalidArg, "null output");
+        *value = rbw::tunedValue(static_cast<rbw::TuneParam>(param), branch_factor, nb_levels, n);
+    });
+}
+
+int rbw_tuning_clear(void)
+{
+    return guard([] { rbw::clearTuning(); });
+}
 
 void rbw_timing_enable(int32_t on) { rbw::timingEnable(on != 0); }
 

@@ -4,6 +4,7 @@
 // Center sums are exact (u32 in shared memory, u64 in global memory).
 #include "kmeans.cuh"
 #include "timing.h"
+#include "tuning.h"
 
 #include <algorithm>
 
@@ -617,10 +618,12 @@ void launchAssign(const KMeansLevel& lv, const NodeTile* tiles, const uint32_t* 
     int dev = 0, sms = 0;
     RBW_CUDA(cudaGetDevice(&dev));
     RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    // A fixed grid: the occupancy query gave one CTA per SM on some launches, 3-4x slower.
+    // A fixed grid (the occupancy query gave one CTA per SM on some launches, 3-4x slower) of
+    // up to kAssignCtasPerSm CTAs per SM, the count the autotuner chose for this workload.
     static_assert(kAssignCtasPerSm * kAssignTmemCols <= 512, "TMEM columns of the resident CTAs");
     static_assert(kAssignCtasPerSm * kAssignSmemBytes <= 227 * 1024, "shared memory of the resident CTAs");
-    const uint32_t grid = std::max(1u, std::min<uint32_t>(maxTiles, static_cast<uint32_t>(sms) * kAssignCtasPerSm));
+    const uint32_t perSm = std::min(kAssignCtasPerSm, tunedValue(kTuneAssignCtasPerSm, lv.B, 0, lv.nbMembers));
+    const uint32_t grid = std::max(1u, std::min<uint32_t>(maxTiles, static_cast<uint32_t>(sms) * perSm));
     ScopedKernelTimer timer(kTimedAssign, s);
     assignKernel<<<grid, kAssignThreads, kAssignSmemBytes, s>>>(lv, tiles, nTilesDev);
     RBW_CUDA(cudaGetLastError());

@@ -19,6 +19,7 @@
 //     sums S_b, counts n_b and sums of squared norms Q_b, with the centers of the assignment.
 #include "kmeans.cuh"
 #include "timing.h"
+#include "tuning.h"
 
 #include <cuda_bf16.h>
 
@@ -484,8 +485,10 @@ void launchAssignF(const KMeansLevelF& lv, const NodeTile* tiles, const uint32_t
                                    attrSet);
     static_assert(kAfCtasPerSm * kAfTmemCols <= 512, "TMEM columns of the resident CTAs");
     static_assert(kAfCtasPerSm * kAfSmemBytes <= 227 * 1024, "shared memory of the resident CTAs");
+    const uint32_t perSm =
+        std::min(kAfCtasPerSm, tunedValue(kTuneAssignFCtasPerSm, lv.base.B, 0, lv.base.nbMembers));
     const uint32_t grid =
-        std::max(1u, std::min<uint32_t>(maxTiles, static_cast<uint32_t>(currentSmCount()) * kAfCtasPerSm));
+        std::max(1u, std::min<uint32_t>(maxTiles, static_cast<uint32_t>(currentSmCount()) * perSm));
     ScopedKernelTimer timer(kTimedAssign, s);
     assignKernelF<<<grid, kAfThreads, kAfSmemBytes, s>>>(lv, tiles, nTilesDev);
     RBW_CUDA(cudaGetLastError());

@@ -15,6 +15,7 @@
 //                     the comparison baseline.  Exact for uint8 data (all sums < 2^24).
 #include "lookup.cuh"
 #include "timing.h"
+#include "tuning.h"
 
 #include <algorithm>
 #include <mutex>
@@ -597,9 +598,10 @@ __global__ void buildTiles(const uint32_t* count, const uint32_t* rowOff, const 
 }
 
 constexpr uint32_t kScatterThreads = 256;
-constexpr uint32_t kScatterPerThread = 16;
 
 // perm[rowOff[node] + rank] = i for every descriptor i (order inside a bin is unspecified).
+// kScatterPerThread rows per thread (8, 16 or 32, chosen by the autotuner).
+template <uint32_t kScatterPerThread>
 __global__ void __launch_bounds__(kScatterThreads) scatterRows(const uint32_t* nodeNext, uint64_t n, uint32_t nb,
                                                                const uint32_t* rowOff, uint32_t* cursor, uint32_t* perm)
 {
@@ -861,9 +863,19 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
             buildTiles<<<tileBlocks, 256, 0, stream>>>(count, rowOff, tileOff, nbBins, totals, maxTiles, tiles);
             RBW_CUDA(cudaGetLastError());
             RBW_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nbBins, stream));
-            const uint64_t per = uint64_t(kScatterThreads) * kScatterPerThread;
-            scatterRows<<<static_cast<uint32_t>((n + per - 1) / per), kScatterThreads, 0, stream>>>(
-                scratch.nodeNext, n, nbBins, rowOff, cursor, scratch.perm);
+            const uint32_t rows = tunedValue(kTuneScatterRows, B, L, n);
+            const uint64_t per = uint64_t(kScatterThreads) * rows;
+            const uint32_t sBlocks = static_cast<uint32_t>((n + per - 1) / per);
+            if (rows == 8) {
+                scatterRows<8><<<sBlocks, kScatterThreads, 0, stream>>>(scratch.nodeNext, n, nbBins, rowOff, cursor,
+                                                                          scratch.perm);
+            } else if (rows == 32) {
+                scatterRows<32><<<sBlocks, kScatterThreads, 0, stream>>>(scratch.nodeNext, n, nbBins, rowOff, cursor,
+                                                                           scratch.perm);
+            } else {
+                scatterRows<16><<<sBlocks, kScatterThreads, 0, stream>>>(scratch.nodeNext, n, nbBins, rowOff, cursor,
+                                                                           scratch.perm);
+            }
             RBW_CUDA(cudaGetLastError());
             kernels += 3;
         }
