@@ -251,6 +251,17 @@ RBW_API int rbw_db_segments(const rbw_database* db, uint32_t* main_docs, uint32_
 /* The stored reciprocal L1 norm of a document's weight vector (DataBase.cpp:54-68). */
 RBW_API int rbw_db_doc_rcp(const rbw_database* db, uint32_t idx_doc, float* rcp);
 
+/* Subtree posting counts of every word, host [levelBeg(L)][B] (the leaf level included), as the
+ * skip rule postings < 16 + 4 max_results (DataBase.cpp:125) uses them; brings the index up to
+ * date first.  No counterpart in the reference. */
+RBW_API int rbw_db_word_postings(const rbw_database* db, uint64_t* host_counts);
+/* Makes the skip rule use host_counts (same layout) instead of this database's own counts; NULL
+ * restores its own.  For a database that holds one shard of a document set: given the counts
+ * summed over all shards, it skips exactly the words the whole set would, so the merged top-k of
+ * the shards equals the top-k of one database holding every document.  Set it again after
+ * documents are added to any shard.  No counterpart in the reference. */
+RBW_API int rbw_db_set_word_postings(rbw_database* db, const uint64_t* host_counts);
+
 /* A leaf's posting list as the reference stores it (DataBase.h:58): document ids ascending,
  * repeated once per descriptor.  *n = full length; at most `capacity` ids are written. */
 RBW_API int rbw_db_postings(const rbw_database* db, uint32_t leaf, uint32_t* out, uint32_t capacity, uint32_t* n);
@@ -300,6 +311,51 @@ RBW_API int rbw_server_reset_stats(rbw_server* server);
 RBW_API int rbw_server_batch_bytes(rbw_server* server, uint64_t n_desc, uint32_t n_requests, uint64_t* bytes);
 /* Fails requests still waiting, finishes the batches in flight. */
 RBW_API void rbw_server_destroy(rbw_server* server);
+
+/* ------------------------------------------------------------------ sharded build
+ * No counterpart in the reference, which builds on one GPU (Vocabulary.cpp:32-121).  One rank's
+ * part of a build whose descriptors are split across ranks (GPUs) in contiguous ranges; the
+ * driver (rapidbow_b200.distributed) runs the same steps on every rank and all-reduces, between
+ * rbw_kmeans_shard_assign and rbw_kmeans_shard_update, the per-node buffers of every Lloyd step:
+ * sums [nodes][16][128] u64, counts [nodes][16] u32 and change counts [nodes] u32 (device
+ * memory, zeroed by the caller before each assign).  The result equals the single-GPU build with
+ * RBW_BUILD_IEEE_DIVISION, byte for byte. */
+typedef struct rbw_kmeans_shard rbw_kmeans_shard;
+RBW_API int rbw_kmeans_shard_create(const void* dev_desc, uint32_t nb_desc, uint32_t branch_factor,
+                                    uint32_t nb_levels, void* stream, rbw_kmeans_shard** out);
+RBW_API void rbw_kmeans_shard_destroy(rbw_kmeans_shard* shard);
+/* Current level and its number of nodes (B^level). */
+RBW_API int rbw_kmeans_shard_level(rbw_kmeans_shard* shard, uint32_t* level, uint32_t* nb_nodes);
+/* Local members of every node of the current level (host [nb_nodes]). */
+RBW_API int rbw_kmeans_shard_node_counts(rbw_kmeans_shard* shard, uint32_t* host_counts);
+/* Rows of local members given as (node, position among the node's local members). */
+RBW_API int rbw_kmeans_shard_member_rows(rbw_kmeans_shard* shard, const uint32_t* host_node,
+                                         const uint32_t* host_pos, uint32_t count, uint8_t* host_rows);
+/* Rows of local descriptors (index within this shard). */
+RBW_API int rbw_kmeans_shard_desc_rows(rbw_kmeans_shard* shard, const uint32_t* host_idx, uint32_t count,
+                                       uint8_t* host_rows);
+/* Initial centers of the current level, host [nb_nodes][B][128]. */
+RBW_API int rbw_kmeans_shard_set_centers(rbw_kmeans_shard* shard, const uint8_t* host_centers);
+/* Local assign step of the nodes whose last reduced change count (dev_last_changed) is non-zero. */
+RBW_API int rbw_kmeans_shard_assign(rbw_kmeans_shard* shard, const uint32_t* dev_last_changed, uint64_t* dev_sums,
+                                    uint32_t* dev_counts, uint32_t* dev_changed);
+/* Update from the reduced buffers (IEEE division, kmeans.cu:356-372); the buffers are only read. */
+RBW_API int rbw_kmeans_shard_update(rbw_kmeans_shard* shard, const uint64_t* dev_sums, const uint32_t* dev_counts,
+                                    const uint32_t* dev_changed);
+RBW_API int rbw_kmeans_shard_get_centers(rbw_kmeans_shard* shard, uint8_t* host_centers);
+/* Stable regroup into the next level (Vocabulary.cpp:83-98); local child counts [nb_nodes][B]. */
+RBW_API int rbw_kmeans_shard_next_level(rbw_kmeans_shard* shard, uint32_t* host_child_counts);
+
+/* The reference's initial picks (kmeans.cpp:141-196) for the nodes of one level, from node sizes:
+ * positions [nb_nodes][B] among each node's members and the number of distinct picks.  One picker
+ * per build: its default-seeded engine carries over from level to level, as in the reference. */
+typedef struct rbw_init_picker rbw_init_picker;
+RBW_API int rbw_init_picker_create(rbw_init_picker** out);
+RBW_API void rbw_init_picker_destroy(rbw_init_picker* picker);
+RBW_API int rbw_init_picker_level(rbw_init_picker* picker, uint32_t branch_factor, const uint32_t* node_counts,
+                                  uint32_t nb_nodes, uint32_t* positions, uint32_t* n_valid);
+/* Node weights from occurrence counts (Vocabulary.cpp:103-108). */
+RBW_API int rbw_idf_weights(uint32_t nb_doc, const uint32_t* occ, uint64_t n, float* weights);
 
 /* ------------------------------------------------------------------ tuning
  * No counterpart in the reference (which sizes its assign grid by an occupancy query,

@@ -86,6 +86,10 @@ class Oracle:
             lib.orc_db_query.restype = C.c_uint32
             lib.orc_db_query.argtypes = [C.c_void_p, u32p, C.c_uint32, C.c_uint32, C.c_int, u32p, f64p,
                                          C.c_uint32]
+            lib.orc_db_word_postings.restype = None
+            lib.orc_db_word_postings.argtypes = [C.c_void_p, u64p]
+            lib.orc_db_set_word_postings.restype = None
+            lib.orc_db_set_word_postings.argtypes = [C.c_void_p, C.c_void_p]
             lib.orc_db_postings.restype = C.c_uint32
             lib.orc_db_postings.argtypes = [C.c_void_p, C.c_uint32, u32p, C.c_uint32]
             Oracle._lib = lib
@@ -188,6 +192,7 @@ class Oracle:
 class OracleDb:
     def __init__(self, orc: Oracle, B: int, L: int, weights: np.ndarray) -> None:
         self.lib = orc.lib
+        self.B, self.L = B, L
         self._w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1)
         self.h = self.lib.orc_db_create(B, L, self._w)
 
@@ -203,6 +208,18 @@ class OracleDb:
 
     def doc_rcp(self, doc: int) -> float:
         return float(self.lib.orc_db_doc_rcp(self.h, doc))
+
+    def word_postings(self) -> np.ndarray:
+        out = np.empty(level_beg(self.B, self.L) * self.B, dtype=np.uint64)
+        self.lib.orc_db_word_postings(self.h, out)
+        return out
+
+    def set_word_postings(self, counts) -> None:
+        if counts is None:
+            self.lib.orc_db_set_word_postings(self.h, None)
+            return
+        self._ext = np.ascontiguousarray(counts, dtype=np.uint64)
+        self.lib.orc_db_set_word_postings(self.h, self._ext.ctypes.data_as(C.c_void_p))
 
     def postings(self, leaf: int) -> np.ndarray:
         n = self.lib.orc_db_postings(self.h, leaf, np.empty(0, np.uint32), 0)

@@ -632,6 +632,7 @@ struct OrcDb {
     std::vector<std::vector<uint32_t>> postings;  // per leaf word, sorted with duplicates
     std::map<uint32_t, float> rcpF;               // DataBase.h:62
     std::map<uint32_t, double> rcpD;              // FP64 restatement
+    std::vector<uint64_t> extWordPost;            // skip-rule counts set from outside (empty: own)
 
     const float* levelWeights(uint32_t level) const { return &weights[levelBeg(B, level) * B]; }
 
@@ -690,6 +691,30 @@ float orc_db_doc_rcp(const void* p, uint32_t idxDoc)
     return it == db->rcpF.end() ? -1.f : it->second;
 }
 
+void orc_db_word_postings(const void* p, uint64_t* out)
+{
+    const auto* db = static_cast<const OrcDb*>(p);
+    for (uint32_t level = 0; level < db->L; level++) {
+        const uint64_t span = ipow(db->B, db->L - 1 - level);
+        const uint64_t words = ipow(db->B, level + 1);
+        for (uint64_t w = 0; w < words; w++) {
+            uint64_t total = 0;
+            for (uint64_t f = w * span; f < (w + 1) * span; f++) total += db->postings[f].size();
+            out[levelBeg(db->B, level) * db->B + w] = total;
+        }
+    }
+}
+
+void orc_db_set_word_postings(void* p, const uint64_t* counts)
+{
+    auto* db = static_cast<OrcDb*>(p);
+    if (counts == nullptr) {
+        db->extWordPost.clear();
+        return;
+    }
+    db->extWordPost.assign(counts, counts + levelBeg(db->B, db->L) * db->B);
+}
+
 uint32_t orc_db_postings(const void* p, uint32_t leaf, uint32_t* out, uint32_t capacity)
 {
     const auto& ivf = static_cast<const OrcDb*>(p)->postings.at(leaf);
@@ -721,7 +746,11 @@ uint32_t orc_db_query(const void* p, const uint32_t* leaves, uint32_t n, uint32_
             const float w = lw[node];
             const uint64_t leafBeg = node * span;
             uint64_t total = 0;
-            for (uint64_t f = leafBeg; f < leafBeg + span; f++) total += db->postings[f].size();
+            if (db->extWordPost.empty()) {
+                for (uint64_t f = leafBeg; f < leafBeg + span; f++) total += db->postings[f].size();
+            } else {
+                total = db->extWordPost[levelBeg(B, level) * B + node];
+            }
             if (level >= L - 1 || total < 16u + uint64_t(maxNbResults) * 4u) { // DataBase.cpp:125
                 std::map<uint32_t, uint32_t> cnt;
                 for (uint64_t f = leafBeg; f < leafBeg + span; f++)

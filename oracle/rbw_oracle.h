@@ -99,6 +99,10 @@ float orc_db_doc_rcp(const void* db, uint32_t idxDoc);
  * docs/scores sorted by (score ascending, doc ascending); returns the count (<= capacity). */
 uint32_t orc_db_query(const void* db, const uint32_t* leaves, uint32_t n, uint32_t maxNbResults,
                       int mode, uint32_t* docs, double* scores, uint32_t capacity);
+/* Subtree posting counts of every word ([levelBeg(L)][B]), and counts the skip rule uses instead
+ * of the database's own (NULL: its own) -- for a database holding one shard of a document set. */
+void orc_db_word_postings(const void* db, uint64_t* out);
+void orc_db_set_word_postings(void* db, const uint64_t* counts);
 /* Postings of one leaf word, sorted ascending with duplicates (= term frequency). */
 uint32_t orc_db_postings(const void* db, uint32_t leaf, uint32_t* out, uint32_t capacity);
 

@@ -99,6 +99,21 @@ def load_library() -> C.CDLL:
         "rbw_voc_get_centers_f32": (C.c_int, [vp, vp]),
         "rbw_voc_build_stats": (C.c_int, [vp, C.POINTER(BuildStats)]),
         "rbw_voc_refined_lookups": (C.c_int, [vp, C.POINTER(u64)]),
+        "rbw_kmeans_shard_create": (C.c_int, [vp, u32, u32, u32, vp, pp]),
+        "rbw_kmeans_shard_destroy": (None, [vp]),
+        "rbw_kmeans_shard_level": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
+        "rbw_kmeans_shard_node_counts": (C.c_int, [vp, vp]),
+        "rbw_kmeans_shard_member_rows": (C.c_int, [vp, vp, vp, u32, vp]),
+        "rbw_kmeans_shard_desc_rows": (C.c_int, [vp, vp, u32, vp]),
+        "rbw_kmeans_shard_set_centers": (C.c_int, [vp, vp]),
+        "rbw_kmeans_shard_assign": (C.c_int, [vp, vp, vp, vp, vp]),
+        "rbw_kmeans_shard_update": (C.c_int, [vp, vp, vp, vp]),
+        "rbw_kmeans_shard_get_centers": (C.c_int, [vp, vp]),
+        "rbw_kmeans_shard_next_level": (C.c_int, [vp, vp]),
+        "rbw_init_picker_create": (C.c_int, [pp]),
+        "rbw_init_picker_destroy": (None, [vp]),
+        "rbw_init_picker_level": (C.c_int, [vp, u32, vp, u32, vp, vp]),
+        "rbw_idf_weights": (C.c_int, [u32, vp, u64, vp]),
         "rbw_tuning_set": (C.c_int, [u32, u32, u32, u32, u32]),
         "rbw_tuning_get": (C.c_int, [u32, u32, u32, u64, C.POINTER(u32)]),
         "rbw_tuning_clear": (C.c_int, []),
@@ -131,6 +146,8 @@ def _bind_optional(lib: C.CDLL) -> None:
         "rbw_db_segments": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
         "rbw_db_doc_rcp": (C.c_int, [vp, u32, C.POINTER(C.c_float)]),
         "rbw_db_postings": (C.c_int, [vp, u32, vp, u32, C.POINTER(u32)]),
+        "rbw_db_word_postings": (C.c_int, [vp, vp]),
+        "rbw_db_set_word_postings": (C.c_int, [vp, vp]),
         "rbw_db_query_batched_host_offsets": (C.c_int, [vp, vp, vp, vp, u32, u32, vp, vp, vp, vp]),
         "rbw_server_options_default": (None, [vp]),
         "rbw_server_create": (C.c_int, [vp, vp, vp, pp]),

@@ -25,7 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
 # --use_fast_math kernels.
 EXTRA = {"kmeans_update.cu": ["--use_fast_math"]}
 SOURCES = ["lookup.cu", "kmeans.cu", "kmeans_update.cu", "kmeans_f32.cu", "vocabulary.cu", "database.cu", "capi.cpp", "facade.cpp",
-           "timing.cpp", "noalloc.cu", "server.cpp", "tuning.cpp"]
+           "timing.cpp", "noalloc.cu", "server.cpp", "tuning.cpp", "kmeans_shard.cu"]
 
 
 def _nvcc() -> str:

@@ -775,7 +775,7 @@ public:
             const size_t prepSmem = size_t(nextPow2(std::max(maxN, 1u))) * 4;
             RBW_CUDA(cudaFuncSetAttribute(queryPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(prepSmem)));
             queryPrepKernel<<<nq, kPrepThreads, prepSmem, stream>>>(
-                dLeaves, dOff, nullptr, nullptr, 0u, mWeights.as<float>(), mWordPost.as<unsigned long long>(), mB, mL,
+                dLeaves, dOff, nullptr, nullptr, 0u, mWeights.as<float>(), skipCounts(), mB, mL,
                 mNbLeaves, k, static_cast<float*>(qr), static_cast<Entry*>(ent), static_cast<uint32_t*>(cnt));
             RBW_CUDA(cudaGetLastError());
             if (!bigQ.empty()) {
@@ -784,7 +784,7 @@ public:
                 uint32_t* gkeys = qList + bigQ.size();
                 RBW_CUDA(cudaMemcpyAsync(qList, bigQ.data(), bigQ.size() * 4, cudaMemcpyHostToDevice, stream));
                 queryPrepKernel<<<static_cast<uint32_t>(bigQ.size()), kPrepThreads, 0, stream>>>(
-                    dLeaves, dOff, qList, gkeys, bigStride, mWeights.as<float>(), mWordPost.as<unsigned long long>(),
+                    dLeaves, dOff, qList, gkeys, bigStride, mWeights.as<float>(), skipCounts(),
                     mB, mL, mNbLeaves, k, static_cast<float*>(qr), static_cast<Entry*>(ent),
                     static_cast<uint32_t*>(cnt));
                 RBW_CUDA(cudaGetLastError());
@@ -832,6 +832,36 @@ public:
         RBW_CUDA(cudaFreeAsync(selG, stream));
         RBW_CUDA(cudaFreeAsync(big, stream));
         recordQuery(stream);
+    }
+
+    // Subtree posting counts of every word ([levelBeg(L)][B], leaf level included) of this
+    // database, as its skip rule uses them.
+    std::vector<uint64_t> wordPostings()
+    {
+        updateIndex();
+        std::shared_lock<std::shared_mutex> lk(mMu);
+        std::vector<uint64_t> out(mNbWords);
+        RBW_CUDA(cudaMemcpyAsync(out.data(), mWordPost.get(), mNbWords * 8, cudaMemcpyDeviceToHost, mStream));
+        RBW_CUDA(cudaStreamSynchronize(mStream));
+        return out;
+    }
+
+    // Counts the skip rule uses instead of this database's own (nullptr: back to its own).  A
+    // database holding one shard of a document set takes the counts summed over all shards, so
+    // every shard skips exactly the words the whole set would (DataBase.cpp:125).
+    void setWordPostings(const uint64_t* host)
+    {
+        std::unique_lock<std::shared_mutex> lk(mMu);
+        if (host == nullptr) {
+            mSkipExternal = false;
+            return;
+        }
+        waitQueriesOnStream();
+        if (mSkipCounts.get() == nullptr) mSkipCounts.reset(mNbWords * 8);
+        RBW_CUDA(cudaMemcpyAsync(mSkipCounts.get(), host, mNbWords * 8, cudaMemcpyHostToDevice, mStream));
+        RBW_CUDA(cudaEventRecord(mIndexReady, mStream));
+        RBW_CUDA(cudaStreamSynchronize(mStream));
+        mSkipExternal = true;
     }
 
     uint32_t nbDocs()
@@ -1060,9 +1090,16 @@ private:
         mIndexed = s1;
     }
 
+    const unsigned long long* skipCounts() const
+    {
+        return mSkipExternal ? mSkipCounts.as<unsigned long long>() : mWordPost.as<unsigned long long>();
+    }
+
     uint32_t mB, mL;
     uint64_t mNbLeaves = 0, mNbWords = 0;
     DeviceBuffer mWeights;
+    DeviceBuffer mSkipCounts;      // counts set by setWordPostings
+    bool mSkipExternal = false;
     // host state
     std::vector<uint32_t> mHostIds;        // slot -> document id
     std::vector<uint64_t> mHostDocOff;     // slot -> first posting (prefix sums of sizes)
@@ -1185,6 +1222,20 @@ int rbw_db_doc_rcp(const rbw_database* db, uint32_t idx_doc, float* rcp)
         if (rcp == nullptr) throw rbw::Error(rbw::kInvalidArg, "null output");
         *rcp = dbOf(db).docRcp(idx_doc);
     });
+}
+
+int rbw_db_word_postings(const rbw_database* db, uint64_t* host_counts)
+{
+    return rbw::runGuarded([&] {
+        if (host_counts == nullptr) throw rbw::Error(rbw::kInvalidArg, "null output");
+        const auto v = dbOf(db).wordPostings();
+        std::memcpy(host_counts, v.data(), v.size() * 8);
+    });
+}
+
+int rbw_db_set_word_postings(rbw_database* db, const uint64_t* host_counts)
+{
+    return rbw::runGuarded([&] { dbOf(db).setWordPostings(host_counts); });
 }
 
 int rbw_db_postings(const rbw_database* db, uint32_t leaf, uint32_t* out, uint32_t capacity, uint32_t* n)

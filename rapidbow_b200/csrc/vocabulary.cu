@@ -114,6 +114,8 @@ __global__ void iotaKernel(uint32_t* p, uint64_t n)
 
 uint32_t blocksFor(uint64_t n, uint32_t t) { return static_cast<uint32_t>((n + t - 1) / t); }
 
+} // namespace
+
 // The reference's initial pick (kmeans.cpp:141-168): min(n, k) distinct members drawn from one
 // default-seeded std::mt19937_64 that lives for the whole build (a fresh thread's
 // thread_local engine), sorted and padded with the last pick.  The steps -- `rng() % n` into a
@@ -143,8 +145,6 @@ float idfWeight(uint32_t nbDoc, uint32_t occ)
     return occ == 0 ? std::numeric_limits<float>::min()
                     : std::max(std::numeric_limits<float>::min(), std::log(float(nbDoc) / float(occ)));
 }
-
-} // namespace
 
 void Vocabulary::allocate(uint32_t B, uint32_t L)
 {

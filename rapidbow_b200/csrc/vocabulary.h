@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <random>
 #include <vector>
 
 namespace rbw {
@@ -133,6 +134,12 @@ private:
 
 // Library-owned stream-ordered memory pool: freed blocks stay cached for the next call.
 cudaMemPool_t libraryPool();
+
+// The reference's initial pick of min(space, k) distinct member positions from `rng`, sorted
+// and padded with the last pick (kmeans.cpp:141-168); returns the number of distinct picks.
+uint32_t referencePick(std::mt19937_64& rng, uint32_t* dst, uint32_t space, uint32_t k);
+// idf-like node weight (Vocabulary.cpp:103-108).
+float idfWeight(uint32_t nbDoc, uint32_t occ);
 
 // Host-to-host lookup: descriptors are copied in and leaf indices copied back in chunks over
 // two streams so transfers overlap the kernels.  Synchronous.  Returns kernels launched.

@@ -92,6 +92,22 @@ class DataBase:
         _check(self._lib.rbw_db_doc_rcp(self._h, doc, C.byref(v)))
         return v.value
 
+    def word_postings(self) -> np.ndarray:
+        """Subtree posting counts of every word ([levelBeg(L) * B] uint64), as the skip rule uses them."""
+        B, L = self.voc.branch_factor, self.voc.nb_levels
+        n = sum(B ** lv for lv in range(L)) * B
+        out = np.empty(n, np.uint64)
+        _check(self._lib.rbw_db_word_postings(self._h, out.ctypes.data))
+        return out
+
+    def set_word_postings(self, counts: Optional[np.ndarray]) -> None:
+        """Counts for the skip rule in place of this database's own (None: its own again)."""
+        if counts is None:
+            _check(self._lib.rbw_db_set_word_postings(self._h, None))
+            return
+        c = np.ascontiguousarray(counts, np.uint64)
+        _check(self._lib.rbw_db_set_word_postings(self._h, c.ctypes.data))
+
     def postings(self, leaf: int) -> np.ndarray:
         n = C.c_uint32()
         _check(self._lib.rbw_db_postings(self._h, leaf, None, 0, C.byref(n)))
