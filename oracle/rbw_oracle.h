@@ -67,7 +67,10 @@ int orc_build_vocabulary(const uint8_t* desc, uint32_t nbDesc, uint32_t nbDoc, u
  *   assign   : argmin of that distance, lowest index on ties (kmeans.cu:131-135);
  *   update   : c = float(double(sum) / double(count)) from exact integer sums, kept when count = 0;
  *   inertia  : FP64 sum over the members of their distance to the assigned center.
- * Initial centers are the same descriptor rows as in the uint8 mode (converted exactly). */
+ * Initial centers are the same descriptor rows as in the uint8 mode (converted exactly).
+ * Parity unpinned: the reference has no float-center mode to run or to take vectors from; this
+ * part is checked against itself (plain FP64 sums, integer trees equal to the uint8 restatement,
+ * independence from the thread count) and shares the uint8 mode's pinned rules. */
 
 /* Squared distance of a uint8 row to an fp32 center: lane l (0..31) forms
  * p_l = fma(e, e, .) over e = double(x[4l+k]) - double(c[4l+k]), k = 0..3 (starting from 0);
