@@ -8,7 +8,9 @@
 // Batching: a dispatcher thread forms a batch from the pending requests, in arrival order, as
 // soon as a batch slot is free, up to the slot's request and descriptor limits and only while
 // the batch's device memory estimate fits the memory budget left by the batches in flight
-// (admission by free HBM).  A batch copies its descriptors in, looks them up and scores all its
+// (admission by free HBM).  A request's descriptors are copied once, at submit, into a pinned
+// buffer from a pool; the batch copies each of its requests to the device straight from there
+// (one asynchronous copy per request), looks them up and scores all its
 // requests in one scoring launch, on its own stream, so up to max_inflight batches overlap on
 // the GPU; requests that arrive meanwhile join the next batch.  A completion thread waits for
 // each batch in order, hands the results to the requests and frees the slot.
@@ -26,6 +28,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -34,9 +37,50 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Pinned host buffers in power-of-two size classes (64 KiB and up), reused across requests, so
+// a request's descriptors are copied once on the host and DMA-copied to the device from there.
+class PinnedPool
+{
+public:
+    ~PinnedPool()
+    {
+        for (auto& cls : mFree)
+            for (void* p : cls) cudaFreeHost(p);
+    }
+    // Returns a buffer of at least `bytes` and its size class.
+    std::pair<uint8_t*, uint32_t> take(size_t bytes)
+    {
+        uint32_t c = 16;
+        while ((size_t(1) << c) < bytes) c++;
+        {
+            std::lock_guard<std::mutex> lk(mMu);
+            if (c < mFree.size() && !mFree[c].empty()) {
+                void* p = mFree[c].back();
+                mFree[c].pop_back();
+                return {static_cast<uint8_t*>(p), c};
+            }
+        }
+        void* p = nullptr;
+        RBW_CUDA(cudaMallocHost(&p, size_t(1) << c));
+        return {static_cast<uint8_t*>(p), c};
+    }
+    void give(uint8_t* p, uint32_t c)
+    {
+        if (p == nullptr) return;
+        std::lock_guard<std::mutex> lk(mMu);
+        if (mFree.size() <= c) mFree.resize(c + 1);
+        mFree[c].push_back(p);
+    }
+
+private:
+    std::mutex mMu;
+    std::vector<std::vector<void*>> mFree;
+};
+
 struct Request {
     uint64_t id = 0;
-    std::vector<uint8_t> desc;   // n x 128
+    uint8_t* desc = nullptr;     // pinned, n x 128 (from the server's pool)
+    uint32_t descClass = 0;
     uint32_t n = 0;
     Clock::time_point submitted, finished;
     bool done = false;
@@ -49,7 +93,6 @@ struct Request {
 struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
-    uint8_t* hDesc = nullptr;     // pinned [maxDesc][128]
     uint64_t* hOff = nullptr;     // pinned [maxQueries + 1]
     uint32_t* hDocs = nullptr;    // pinned [maxQueries][k]
     float* hScores = nullptr;     // pinned [maxQueries][k]
@@ -84,7 +127,6 @@ public:
         for (Slot& s : mSlots) {
             RBW_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
             RBW_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
-            RBW_CUDA(cudaMallocHost(&s.hDesc, mOpt.max_batch_descriptors * 128));
             RBW_CUDA(cudaMallocHost(&s.hOff, (q + 1) * 8));
             RBW_CUDA(cudaMallocHost(&s.hDocs, q * k * 4));
             RBW_CUDA(cudaMallocHost(&s.hScores, q * k * 4));
@@ -105,7 +147,6 @@ public:
         mCompleter.join();
         for (Slot& s : mSlots) {
             cudaStreamSynchronize(s.stream);
-            cudaFreeHost(s.hDesc);
             cudaFreeHost(s.hOff);
             cudaFreeHost(s.hDocs);
             cudaFreeHost(s.hScores);
@@ -121,7 +162,10 @@ public:
         if (n > mOpt.max_batch_descriptors) throw Error(kInvalidArg, "request larger than a batch");
         if (estimate(n, 1) > mOpt.hbm_budget_bytes) throw Error(kOutOfMemory, "request larger than the memory budget");
         auto r = std::make_shared<Request>();
-        r->desc.assign(desc, desc + size_t(n) * 128);
+        if (n) {
+            std::tie(r->desc, r->descClass) = mPinned.take(size_t(n) * 128);
+            std::memcpy(r->desc, desc, size_t(n) * 128);
+        }
         r->n = n;
         std::lock_guard<std::mutex> lk(mMu);
         if (mStop) throw Error(kInvalidArg, "server stopped");
@@ -299,7 +343,6 @@ private:
         uint64_t off = 0;
         for (uint32_t i = 0; i < nq; i++) {
             s.hOff[i] = off;
-            if (s.reqs[i]->n) std::memcpy(s.hDesc + off * 128, s.reqs[i]->desc.data(), size_t(s.reqs[i]->n) * 128);
             off += s.reqs[i]->n;
         }
         s.hOff[nq] = off;
@@ -315,7 +358,12 @@ private:
             uint32_t* dDocs = reinterpret_cast<uint32_t*>(dOff + nq + 1);
             float* dScores = reinterpret_cast<float*>(dDocs + size_t(nq) * k);
             uint32_t* dCount = reinterpret_cast<uint32_t*>(dScores + size_t(nq) * k);
-            if (desc) RBW_CUDA(cudaMemcpyAsync(dDesc, s.hDesc, desc * 128, cudaMemcpyHostToDevice, s.stream));
+            for (uint32_t i = 0; i < nq; i++) {
+                const Request& r = *s.reqs[i];
+                if (r.n)
+                    RBW_CUDA(cudaMemcpyAsync(dDesc + s.hOff[i] * 128, r.desc, size_t(r.n) * 128,
+                                             cudaMemcpyHostToDevice, s.stream));
+            }
             RBW_CUDA(cudaMemcpyAsync(dOff, s.hOff, (size_t(nq) + 1) * 8, cudaMemcpyHostToDevice, s.stream));
             uint32_t kernels = 0;
             int rc = desc ? rbw_voc_lookup_ex(mVoc, dDesc, desc, dLeaf, RBW_LOOKUP_AUTO, s.stream, &kernels) : RBW_OK;
@@ -380,12 +428,14 @@ private:
         r.error = err;
         r.finished = Clock::now();
         r.done = true;
-        r.desc.clear();
-        r.desc.shrink_to_fit();
+        // the batch that copied these descriptors has completed (or never ran)
+        mPinned.give(r.desc, r.descClass);
+        r.desc = nullptr;
         if (status == RBW_OK)
             mLatencies.push_back(std::chrono::duration<double, std::milli>(r.finished - r.submitted).count());
     }
 
+    PinnedPool mPinned; // destroyed after the threads (declared before them)
     const rbw_vocabulary* mVoc;
     rbw_database* mDb;
     rbw_server_options mOpt;
