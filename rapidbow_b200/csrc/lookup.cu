@@ -146,6 +146,103 @@ __device__ __forceinline__ uint32_t argminScores(const uint32_t (&dot)[16], cons
     return bi;
 }
 
+// Four 8x8 b16 matrices from shared memory (lanes 8i..8i+7 give the row addresses of matrix i);
+// register i of a thread holds row lane/4, bytes 4 (lane % 4) .. + 3 of matrix i.
+__device__ __forceinline__ void ldsmX4(uint32_t addr, uint32_t (&r)[4])
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr)
+                 : "memory");
+}
+// d += a (16x32 u8, row-major) * b (32x8 u8, column-major), s32 accumulators (warp-level MMA).
+__device__ __forceinline__ void mmaSyncU8(int32_t (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                 "{%0, %1, %2, %3};"
+                 : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Node-level branch of the warp's 32 tile rows (rows 32 q .. 32 q + 31 of the 128-row tile at
+// shared address aBase), with the node's 16 centers at bBase -- both in the 128-byte swizzled
+// K-major layout -- by warp-level MMAs (2 row blocks x 2 center blocks x 4 K steps of 32), so the
+// tensor memory stays free for the children.  Returns the branch of row 32 q + lane:
+// argmin_b (|c_b|^2 - 2 x.c_b), lowest b on ties (vocTreeLookUp.cu:108-125).
+__device__ __forceinline__ uint32_t warpNodeArgmin(uint32_t aBase, uint32_t bBase, uint32_t q, uint32_t lane,
+                                                   const int32_t* cnormNode)
+{
+    const uint32_t mi = lane >> 3, r8 = lane & 7u;
+    uint32_t res[2][2];
+#pragma unroll
+    for (uint32_t m = 0; m < 2; m++) {
+        // rows 32 q + 16 m .. + 15 against the 16 centers, K in four steps of 32 bytes
+        int32_t d[2][4];
+#pragma unroll
+        for (int n = 0; n < 2; n++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) d[n][e] = 0;
+#pragma unroll
+        for (uint32_t kk = 0; kk < 4; kk++) {
+            // centers: matrix mi = (centers 8 (mi / 2) .. +7, bytes 16 (mi % 2) of K step kk)
+            uint32_t bf[4];
+            {
+                const uint32_t c = 8u * (mi >> 1) + r8;
+                const uint32_t chunk = 2u * kk + (mi & 1u);
+                ldsmX4(bBase + c * 128u + ((chunk ^ (c & 7u)) << 4), bf);
+            }
+            // rows: matrix mi = (rows 16 m + 8 (mi % 2) .. +7, bytes 16 (mi / 2) of K step kk)
+            uint32_t af[4];
+            {
+                const uint32_t row = 32u * q + 16u * m + 8u * (mi & 1u) + r8;
+                const uint32_t chunk = 2u * kk + (mi >> 1);
+                ldsmX4(aBase + row * 128u + ((chunk ^ (row & 7u)) << 4), af);
+            }
+            mmaSyncU8(d[0], af, bf[0], bf[1]);
+            mmaSyncU8(d[1], af, bf[2], bf[3]);
+        }
+        // thread holds rows {16 m + lane/4 + 8 h} x centers {8 n + 2 (lane % 4) + e}: d[n][2 h + e]
+#pragma unroll
+        for (uint32_t h = 0; h < 2; h++) {
+            int32_t best = 0x7FFFFFFF;
+            uint32_t bi = 0;
+#pragma unroll
+            for (uint32_t n = 0; n < 2; n++) {
+#pragma unroll
+                for (uint32_t e = 0; e < 2; e++) {
+                    const uint32_t c = 8u * n + 2u * (lane & 3u) + e;
+                    const int32_t s = cnormNode[c] - 2 * d[n][2 * h + e];
+                    if (s < best) {
+                        best = s;
+                        bi = c;
+                    }
+                }
+            }
+            // the four lanes of a quad hold the row's 16 centers: lowest score, then lowest index
+#pragma unroll
+            for (uint32_t off = 1; off <= 2; off <<= 1) {
+                const int32_t ob = __shfl_xor_sync(0xFFFFFFFFu, best, off);
+                const uint32_t oi = __shfl_xor_sync(0xFFFFFFFFu, bi, off);
+                if (ob < best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            res[m][h] = bi;
+        }
+    }
+    // row 32 q + lane was computed by quad lane % 8 as (m, h) = (lane / 16, (lane / 8) % 2)
+    uint32_t mine = 0;
+#pragma unroll
+    for (uint32_t m = 0; m < 2; m++)
+#pragma unroll
+        for (uint32_t h = 0; h < 2; h++) {
+            const uint32_t v = __shfl_sync(0xFFFFFFFFu, res[m][h], 4u * (lane & 7u));
+            if ((lane >> 4) == m && ((lane >> 3) & 1u) == h) mine = v;
+        }
+    return mine;
+}
+
 // Tile i of this CTA (first pass: computed; later passes: the staged copy of the tile list).
 __device__ __forceinline__ TileInfo tileAtSmem(const TcSmem& S, const PassParams& p, uint32_t t0, uint32_t i)
 {
@@ -172,6 +269,13 @@ __device__ __forceinline__ void emitRow(TcSmem& S, const PassParams& p, bool sme
     }
 }
 
+// kWarpNode = false: both levels on tcgen05, the node-level MMA and the children MMA of a tile in
+// the same TMEM buffer (the children MMA waits until the team has read the node level).
+// kWarpNode = true: the epilogue teams take the node level from the shared-memory tile with
+// warp-level MMAs (warpNodeArgmin) while the children MMA runs, which is then issued as soon as
+// the tile has landed and its buffer is free; a tile slot is released once both its children MMA
+// and the team's reads are done.
+template <bool kWarpNode>
 __global__ void __launch_bounds__(kTcThreads, 1)
     lookupPassTc(const __grid_constant__ CUtensorMap tmapTile, const PassParams p)
 {
@@ -192,7 +296,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < kStages; s++) {
             mbarInit(&S.aFull[s], 1);
-            mbarInit(&S.aEmpty[s], 1);
+            // kWarpNode: the children MMA's commit (two levels) and the four warps of the team
+            mbarInit(&S.aEmpty[s], kWarpNode ? (two ? 1u : 0u) + kTeamWarps : 1u);
         }
         for (uint32_t j = 0; j < 2; j++) {
             mbarInit(&S.bFull[j], 1);
@@ -373,7 +478,25 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (!mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 20)) break;
                     prevGroup = ti.group;
                 }
-                if ((t & 1u) == jm) {
+                if constexpr (kWarpNode) {
+                    // children only: as soon as the tile has landed and team j has read the
+                    // buffer's previous tile
+                    if ((t & 1u) == jm && two) {
+                        const uint32_t s = t % kStages;
+                        if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21)) break;
+                        if (t >= 2 && !mbarWait(&S.bufFree[jm], ((t >> 1) - 1u) & 1u, abortFlag, p.err, 25)) break;
+                        tcFenceAfter();
+                        const uint32_t aBase = smemAddr(S.a[s]);
+                        const uint32_t bBase = smemAddr(S.b[slot]);
+#pragma unroll
+                        for (uint32_t q4 = 0; q4 < 4; q4++) {
+                            mmaU8(tmem + kTmemBuf * jm, smemDescSw128(aBase + 32u * q4),
+                                  smemDescSw128(bBase + kNodeBytes + 32u * q4), idescB, q4 > 0 ? 1u : 0u);
+                        }
+                        mmaCommit(&S.accB[jm]);
+                        mmaCommit(&S.aEmpty[s]);
+                    }
+                } else if ((t & 1u) == jm) {
                     const uint32_t j = jm;
                     const uint32_t s = t % kStages;
                     if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 21)) break;
@@ -439,18 +562,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (j == team) {
                 const uint32_t orig = row < ti.count ? (gather ? __ldg(p.perm + ti.start + row) : ti.start + row) : 0u;
                 const uint32_t base = tRow + kTmemBuf * j;
-                if (!mbarWait(&S.accA[j], (t >> 1) & 1u, abortFlag, p.err, 30)) break;
-                tcFenceAfter();
                 uint32_t b;
-                {
-                    uint32_t r[16];
-                    tmemLoad16(base, r);
-                    tmemWaitTie(r);
-                    b = argminScores(r, &S.cn[slot][0][0]);
+                if constexpr (kWarpNode) {
+                    // node level from the shared-memory tile (warp-level MMAs), while the
+                    // children MMA of the same tile runs on the tensor core
+                    const uint32_t s = t % kStages;
+                    if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 34)) break;
+                    b = warpNodeArgmin(smemAddr(S.a[s]), smemAddr(S.b[slot]), q, lane, &S.cn[slot][0][0]);
+                    __syncwarp();
+                    if (lane == 0) mbarArrive(&S.aEmpty[s]); // this warp is done reading the tile
+                } else {
+                    if (!mbarWait(&S.accA[j], (t >> 1) & 1u, abortFlag, p.err, 30)) break;
+                    tcFenceAfter();
+                    {
+                        uint32_t r[16];
+                        tmemLoad16(base, r);
+                        tmemWaitTie(r);
+                        b = argminScores(r, &S.cn[slot][0][0]);
+                    }
+                    tcFenceBefore();
+                    __syncwarp();
+                    if (lane == 0) mbarArrive(two ? &S.aRead[j] : &S.bufFree[j]);
                 }
-                tcFenceBefore();
-                __syncwarp();
-                if (lane == 0) mbarArrive(two ? &S.aRead[j] : &S.bufFree[j]);
                 if (!two) {
                     if (row < ti.count) emitRow(S, p, smemHist, orig, ti.group * p.B + b);
                 } else {
@@ -471,10 +604,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     };
                     pick(0);
                     pick(1);
-                    // columns [0, 128) have been read: the level-2p MMA of tile t + 2 may start
-                    tcFenceBefore();
-                    __syncwarp();
-                    if (lane == 0) mbarArrive(&S.lowFree[j]);
+                    if constexpr (!kWarpNode) {
+                        // columns [0, 128) have been read: the level-2p MMA of tile t + 2 may start
+                        tcFenceBefore();
+                        __syncwarp();
+                        if (lane == 0) mbarArrive(&S.lowFree[j]);
+                    }
                     if (p.B > 8) {
                         pick(2);
                         pick(3);
@@ -806,9 +941,15 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
         RBW_CUDA(cudaGetLastError());
         return 1;
     }
-    static std::atomic<uint64_t> attrSet{0};
-    setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(lookupPassTc), static_cast<int>(kTcSmemBytes),
-                                   attrSet);
+    const bool warpNode = algo == kLookupTensorU8WarpNode;
+    static std::atomic<uint64_t> attrSet{0}, attrSetW{0};
+    if (warpNode) {
+        setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(lookupPassTc<true>),
+                                       static_cast<int>(kTcSmemBytes), attrSetW);
+    } else {
+        setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(lookupPassTc<false>),
+                                       static_cast<int>(kTcSmemBytes), attrSet);
+    }
     const CUtensorMap tmapTile = makeRowMap(desc, n, kTileRows);
     const uint32_t B = tree.B, L = tree.L;
     const uint32_t passes = (L + 1) / 2;
@@ -851,7 +992,11 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
         }
         {
             ScopedKernelTimer timer(kTimedLookupPass, stream);
-            lookupPassTc<<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
+            if (warpNode) {
+                lookupPassTc<true><<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
+            } else {
+                lookupPassTc<false><<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
+            }
             RBW_CUDA(cudaGetLastError());
         }
         kernels++;

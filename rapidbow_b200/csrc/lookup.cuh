@@ -19,6 +19,7 @@ enum LookupAlgo : int {
     kLookupAuto = 0,     // fastest exact path (tensor cores)
     kLookupTensorU8 = 1, // tcgen05 kind::i8, level pairs + counting-sort regroup
     kLookupSimtF32 = 2,  // plain FP32 SIMT kernel (the comparison baseline)
+    kLookupTensorU8WarpNode = 3, // as kLookupTensorU8, the node level of each pair by warp-level MMAs
 };
 
 struct LookupStats {
