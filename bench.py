@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--n", type=int, default=N_LOOKUP)
+    p.add_argument("--algo", default="auto", choices=["auto", "tensor_u8", "tensor_u8_warpnode"],
+                   help="tensor-core lookup variant of the timed steps (auto = the library's default)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -277,7 +279,7 @@ def run_ours(args, world, rank, local):
         tuned = {"param": "scatter_rows", "value": e["value"], "default": 16, "tuned_ms": e["ms"],
                  "default_ms": e["default_ms"], "kernel": "scanBins + buildTiles + scatterRows (per lookup)"}
     with ClockSampler(local) as clocks:
-        ms, launches, (k_ms, k_n) = timed("tensor_u8", args.steps, args.warmup, "lookup_pass_tc")
+        ms, launches, (k_ms, k_n) = timed(args.algo, args.steps, args.warmup, "lookup_pass_tc")
     clk = clocks.summary()
     ms_simt, _, (s_ms, s_n) = timed("simt_f32", max(3, args.steps // 4), 2, "lookup_simt_f32")
     # exactness on the bench data: tensor-core IDs == FP32 kernel IDs
@@ -297,7 +299,7 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": WORKLOAD, "descriptors_per_gpu": n, "branching": B, "levels": L,
                    "parallelism": f"dp{world} (tree replicated, descriptors sharded)",
-                   "l2": "inputs 1.28 GB per GPU > 126 MB L2, no flush needed", "algo": "tensor_u8"},
+                   "l2": "inputs 1.28 GB per GPU > 126 MB L2, no flush needed", "algo": args.algo},
         "gpu_launches": launches,
         "bit_exact_vs_fp32_kernel": same,
         "refined_descriptors": 0,
