@@ -260,17 +260,22 @@ __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* 
                                                                 uint32_t gstride, const float* weights,
                                                                 const unsigned long long* wordPost, uint32_t B,
                                                                 uint32_t L, uint64_t nbLeaves, uint32_t k,
-                                                                float* qRcpF, Entry* entries, uint32_t* entryCount)
+                                                                float* qRcpF, Entry* entries, uint32_t* entryCount,
+                                                                unsigned long long* work)
 {
     extern __shared__ uint32_t skeys[];
     __shared__ uint32_t cnt, nValid;
+    __shared__ unsigned long long workSum;
     const uint32_t q = gkeys ? qList[blockIdx.x] : blockIdx.x;
     const uint64_t beg = qOff[q];
     const uint32_t nAll = static_cast<uint32_t>(qOff[q + 1] - beg);
     if (gkeys == nullptr && nAll > kMaxDocDesc) return; // prepared by the global-memory launch
     uint32_t* keys = gkeys ? gkeys + uint64_t(blockIdx.x) * gstride : skeys;
     Entry* out = entries + (beg - qOff[0]) * L;
-    if (threadIdx.x == 0) cnt = 0;
+    if (threadIdx.x == 0) {
+        cnt = 0;
+        workSum = 0;
+    }
     const uint32_t n = loadAndSort(qLeaves + beg, nAll, keys, nbLeaves, &nValid);
     if (threadIdx.x < 32) {
         const double norm = l1NormWarp(keys, n, weights, B, L);
@@ -297,13 +302,36 @@ __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* 
                 if (it == 0 || wordPost[widx] < limit) {
                     const uint32_t p = atomicAdd(&cnt, 1u);
                     out[p] = Entry{level, word, run, static_cast<uint32_t>(widx)};
+                    atomicAdd(&workSum, wordPost[widx] + 1ull); // postings the scoring will read
                 }
             }
         }
         span *= B;
     }
     __syncthreads();
-    if (threadIdx.x == 0) entryCount[q] = cnt;
+    if (threadIdx.x == 0) {
+        entryCount[q] = cnt;
+        work[q] = workSum;
+    }
+}
+
+constexpr uint32_t kOrderMax = 4096; // batches up to this many queries are launched by work
+
+// order[] = the queries by descending work (ties by ascending index), so the scoring launch
+// starts the longest queries first and the last wave holds the short ones.  One CTA.
+__global__ void __launch_bounds__(1024) workOrderKernel(const unsigned long long* work, uint32_t nq, uint32_t* order)
+{
+    __shared__ unsigned long long keys[kOrderMax];
+    uint32_t nPow2 = 1;
+    while (nPow2 < nq) nPow2 <<= 1;
+    for (uint32_t i = threadIdx.x; i < nPow2; i += blockDim.x) {
+        // ascending sort of (~work << 32 | index): descending work, then ascending index
+        const unsigned long long w = i < nq ? (work[i] > 0xFFFFFFFEull ? 0xFFFFFFFEull : work[i]) : 0ull;
+        keys[i] = i < nq ? ((0xFFFFFFFFull - w) << 32) | i : ~0ull;
+    }
+    __syncthreads();
+    bitonicSortShared(keys, nPow2);
+    for (uint32_t i = threadIdx.x; i < nq; i += blockDim.x) order[i] = static_cast<uint32_t>(keys[i]);
 }
 
 struct SegmentView {
@@ -328,6 +356,7 @@ struct ScoreParams {
     uint32_t k;
     unsigned long long* cand;  // [nq][shards][k] candidate keys when there are several shards
     unsigned long long* selGlobal; // k > kMaxK: [nq][shards][selStride] selection buffers
+    const uint32_t* order;     // launch order of the queries (nullptr: in index order)
     uint32_t selStride;        // power of two >= k
     uint32_t* outDocs;         // [nq][k]
     float* outScores;          // [nq][k]
@@ -429,7 +458,7 @@ __global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
     extern __shared__ unsigned long long dyn[];
     __shared__ uint32_t nTouched;
     __shared__ unsigned long long sel[kMaxK];
-    const uint32_t q = blockIdx.x;
+    const uint32_t q = P.order ? P.order[blockIdx.x] : blockIdx.x;
     const uint32_t shard = blockIdx.y;
     const uint32_t docBeg = kSharded ? shard * P.shardDocs : 0u;
     const uint32_t nLocal = kSharded ? min(P.shardDocs, P.nDocs - docBeg) : P.nDocs;
@@ -764,6 +793,10 @@ public:
         const uint32_t bigStride = maxBig ? nextPow2(maxBig) : 0u;
         const size_t bigBytes = bigQ.empty() ? 16 : bigQ.size() * (size_t(bigStride) + 1) * 4;
         void *ent = nullptr, *cnt = nullptr, *qr = nullptr, *cand = nullptr, *selG = nullptr, *big = nullptr;
+        void* wk = nullptr;
+        RBW_CUDA(cudaMallocFromPoolAsync(&wk, size_t(nq) * 12, pool, stream));
+        unsigned long long* work = static_cast<unsigned long long*>(wk);
+        uint32_t* order = reinterpret_cast<uint32_t*>(work + nq);
         RBW_CUDA(cudaMallocFromPoolAsync(&ent, entBytes, pool, stream));
         RBW_CUDA(cudaMallocFromPoolAsync(&cnt, size_t(nq) * 4, pool, stream));
         RBW_CUDA(cudaMallocFromPoolAsync(&qr, size_t(nq) * 4, pool, stream));
@@ -776,7 +809,7 @@ public:
             RBW_CUDA(cudaFuncSetAttribute(queryPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(prepSmem)));
             queryPrepKernel<<<nq, kPrepThreads, prepSmem, stream>>>(
                 dLeaves, dOff, nullptr, nullptr, 0u, mWeights.as<float>(), skipCounts(), mB, mL,
-                mNbLeaves, k, static_cast<float*>(qr), static_cast<Entry*>(ent), static_cast<uint32_t*>(cnt));
+                mNbLeaves, k, static_cast<float*>(qr), static_cast<Entry*>(ent), static_cast<uint32_t*>(cnt), work);
             RBW_CUDA(cudaGetLastError());
             if (!bigQ.empty()) {
                 // queries above kMaxDocDesc descriptors: one CTA each, sorted in global memory
@@ -786,7 +819,7 @@ public:
                 queryPrepKernel<<<static_cast<uint32_t>(bigQ.size()), kPrepThreads, 0, stream>>>(
                     dLeaves, dOff, qList, gkeys, bigStride, mWeights.as<float>(), skipCounts(),
                     mB, mL, mNbLeaves, k, static_cast<float*>(qr), static_cast<Entry*>(ent),
-                    static_cast<uint32_t*>(cnt));
+                    static_cast<uint32_t*>(cnt), work);
                 RBW_CUDA(cudaGetLastError());
             }
             ScoreParams P{};
@@ -808,6 +841,15 @@ public:
             P.cand = shards > 1 ? static_cast<unsigned long long*>(cand) : nullptr;
             P.selGlobal = k > kMaxK ? static_cast<unsigned long long*>(selG) : nullptr;
             P.selStride = selStride;
+            // more queries than one wave of scoring CTAs: start the longest ones first
+            int dev = 0, sms = 0;
+            RBW_CUDA(cudaGetDevice(&dev));
+            RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            if (nq > uint32_t(sms) && nq <= kOrderMax) {
+                workOrderKernel<<<1, 1024, 0, stream>>>(work, nq, order);
+                RBW_CUDA(cudaGetLastError());
+                P.order = order;
+            }
             P.outDocs = dDocs;
             P.outScores = dScores;
             P.outCount = dCount;
@@ -831,6 +873,7 @@ public:
         RBW_CUDA(cudaFreeAsync(cand, stream));
         RBW_CUDA(cudaFreeAsync(selG, stream));
         RBW_CUDA(cudaFreeAsync(big, stream));
+        RBW_CUDA(cudaFreeAsync(wk, stream));
         recordQuery(stream);
     }
 
