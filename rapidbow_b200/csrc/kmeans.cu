@@ -378,16 +378,30 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignCtasPerSm) assignKernel
     tcFenceAfter();
     const uint32_t tmem = S.tmemBase;
     uint32_t curNode = 0xFFFFFFFFu, phase = 0;
+    bool curExclusive = false; // every tile of the current node is in this CTA's range
     auto flush = [&]() {
         __syncthreads();
         if (curNode != 0xFFFFFFFFu) {
+            // A node no other CTA touches in this launch is written with plain stores (its
+            // global accumulators are zero on entry); a shared node is added atomically.
             for (uint32_t i = tid; i < kMaxBranch * kDims; i += kAssignThreads) {
                 const uint32_t b = i / kDims, d = i % kDims;
                 const uint32_t v = S.acc[accIndex(b, d)];
-                if (v) atomicAdd(lv.sums + (uint64_t(curNode) * kMaxBranch + b) * kDims + d, (unsigned long long)v);
+                unsigned long long* dst = lv.sums + (uint64_t(curNode) * kMaxBranch + b) * kDims + d;
+                if (v) {
+                    if (curExclusive) *dst = v;
+                    else atomicAdd(dst, (unsigned long long)v);
+                }
             }
-            if (tid < kMaxBranch && S.cnt[tid]) atomicAdd(lv.counts + uint64_t(curNode) * kMaxBranch + tid, S.cnt[tid]);
-            if (tid == 0 && S.chg) atomicAdd(lv.changed + curNode, S.chg);
+            if (tid < kMaxBranch && S.cnt[tid]) {
+                uint32_t* dst = lv.counts + uint64_t(curNode) * kMaxBranch + tid;
+                if (curExclusive) *dst = S.cnt[tid];
+                else atomicAdd(dst, S.cnt[tid]);
+            }
+            if (tid == 0 && S.chg) {
+                if (curExclusive) lv.changed[curNode] = S.chg;
+                else atomicAdd(lv.changed + curNode, S.chg);
+            }
         }
         __syncthreads();
     };
@@ -397,6 +411,7 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignCtasPerSm) assignKernel
         if (ti.node != curNode) {
             flush();
             curNode = ti.node;
+            curExclusive = ti.first >= t0 && uint64_t(ti.first) + (lv.nodeCnt[curNode] + kAssignRows - 1) / kAssignRows <= t1;
             {
                 // thread i copies chunk i % 8 of center i / 8 (16 centers x 8 chunks)
                 const uint32_t b = tid / 8, c = tid % 8;

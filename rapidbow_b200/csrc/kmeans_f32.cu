@@ -173,19 +173,35 @@ __global__ void __launch_bounds__(kAfThreads, kAfCtasPerSm) assignKernelF(KMeans
     tcFenceAfter();
     const uint32_t tmem = S.tmemBase;
     uint32_t curNode = 0xFFFFFFFFu, phase = 0;
+    bool curExclusive = false; // every tile of the current node is in this CTA's range
     auto flush = [&]() {
         __syncthreads();
         if (curNode != 0xFFFFFFFFu && build) {
+            // plain stores for a node no other CTA touches (its accumulators are zero on entry)
             for (uint32_t i = tid; i < kMaxBranch * kDims; i += kAfThreads) {
                 const uint32_t b = i / kDims, d = i % kDims;
                 const uint32_t v = S.acc[accIndexF(b, d)];
-                if (v) atomicAdd(L0.sums + (uint64_t(curNode) * kMaxBranch + b) * kDims + d, (unsigned long long)v);
+                unsigned long long* dst = L0.sums + (uint64_t(curNode) * kMaxBranch + b) * kDims + d;
+                if (v) {
+                    if (curExclusive) *dst = v;
+                    else atomicAdd(dst, (unsigned long long)v);
+                }
             }
             if (tid < kMaxBranch && S.cnt[tid]) {
-                atomicAdd(L0.counts + uint64_t(curNode) * kMaxBranch + tid, S.cnt[tid]);
-                atomicAdd(lv.q + uint64_t(curNode) * kMaxBranch + tid, S.q[tid]);
+                uint32_t* c = L0.counts + uint64_t(curNode) * kMaxBranch + tid;
+                unsigned long long* qd = lv.q + uint64_t(curNode) * kMaxBranch + tid;
+                if (curExclusive) {
+                    *c = S.cnt[tid];
+                    *qd = S.q[tid];
+                } else {
+                    atomicAdd(c, S.cnt[tid]);
+                    atomicAdd(qd, S.q[tid]);
+                }
             }
-            if (tid == 0 && S.chg) atomicAdd(L0.changed + curNode, S.chg);
+            if (tid == 0 && S.chg) {
+                if (curExclusive) L0.changed[curNode] = S.chg;
+                else atomicAdd(L0.changed + curNode, S.chg);
+            }
         }
         __syncthreads();
     };
@@ -196,6 +212,7 @@ __global__ void __launch_bounds__(kAfThreads, kAfCtasPerSm) assignKernelF(KMeans
         if (ti.node != curNode) {
             flush();
             curNode = ti.node;
+            curExclusive = ti.first >= t0 && uint64_t(ti.first) + (L0.nodeCnt[curNode] + kAfRows - 1) / kAfRows <= t1;
             const uint4* src = reinterpret_cast<const uint4*>(lv.split + uint64_t(curNode) * kSplitBytes);
 #pragma unroll
             for (uint32_t k = 0; k < kSplitBytes / 16 / kAfThreads; k++)
