@@ -302,7 +302,10 @@ def test_edge_cases(oracle):
     db.add_doc(11, np.array([9, 9], np.uint32))
     assert 11 in db.query(np.array([9, 9], np.uint32), 10).tolist()
     # max_results beyond every touched document: all of them (no limit on k)
-    assert np.array_equal(db.query(np.array([9, 5], np.uint32), 5000), got)
+    odb.add(11, np.array([9, 9], np.uint32))
+    odocs, _ = odb.query(np.array([9, 5], np.uint32), 5000)
+    assert np.array_equal(db.query(np.array([9, 5], np.uint32), 5000), odocs)
+    assert odocs.size == 3
 
 
 def test_incremental_segments_match_oracle(oracle):

@@ -72,7 +72,8 @@ def test_float_lookup_near_ties_match_fp64_oracle(oracle):
     refined = voc.refined_lookups()
     want = oracle.lookup_f32(centers, B, L, desc, threads=THREADS)
     assert np.array_equal(got, want), f"{np.count_nonzero(got != want)} of {got.size} differ"
-    assert 0 < refined < 3 * desc.shape[0]
+    # every center has a near copy, so nearly every descriptor is re-scored at every level
+    assert 0.5 * 3 * desc.shape[0] < refined <= 3 * desc.shape[0]
 
 
 def test_float_blob_round_trip_and_rounded_tree():
