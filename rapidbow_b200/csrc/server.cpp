@@ -64,6 +64,17 @@ public:
         RBW_CUDA(cudaMallocHost(&p, size_t(1) << c));
         return {static_cast<uint8_t*>(p), c};
     }
+    // Fills each size class from 2^lo to 2^hi bytes with `count` buffers ahead of time, so the
+    // first requests do not wait for page-locked allocations.
+    void reserve(uint32_t lo, uint32_t hi, uint32_t count)
+    {
+        for (uint32_t c = lo; c <= hi; c++)
+            for (uint32_t k = 0; k < count; k++) {
+                void* p = nullptr;
+                RBW_CUDA(cudaMallocHost(&p, size_t(1) << c));
+                give(static_cast<uint8_t*>(p), c);
+            }
+    }
     void give(uint8_t* p, uint32_t c)
     {
         if (p == nullptr) return;
@@ -131,6 +142,12 @@ public:
             RBW_CUDA(cudaMallocHost(&s.hDocs, q * k * 4));
             RBW_CUDA(cudaMallocHost(&s.hScores, q * k * 4));
             RBW_CUDA(cudaMallocHost(&s.hCount, q * 4));
+        }
+        {
+            // requests of up to 8,192 descriptors find a pinned buffer ready
+            uint32_t hi = 16;
+            while (hi < 20 && (size_t(1) << hi) < mOpt.max_batch_descriptors * 128) hi++;
+            mPinned.reserve(16, hi, 8);
         }
         mDispatcher = std::thread([this] { dispatchLoop(); });
         mCompleter = std::thread([this] { completeLoop(); });
@@ -253,16 +270,23 @@ private:
     }
 
     // Device memory free right now: the driver's free memory plus what the library's pool holds
-    // unused (memory freed by finished batches stays in the pool for the next ones).
-    size_t liveFreeBytes() const
+    // unused (memory freed by finished batches stays in the pool for the next ones).  The driver
+    // is asked at most every kLiveRefresh; in between, the value goes down by what the batches
+    // admitted since then reserve.
+    static constexpr std::chrono::microseconds kLiveRefresh{500};
+    size_t liveFreeBytes()
     {
+        const auto now = Clock::now();
+        if (now - mLiveAt < kLiveRefresh) return mLiveFree;
         size_t freeB = 0, totalB = 0;
         if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) return 0;
         cudaMemPool_t pool = libraryPool();
         uint64_t reserved = 0, used = 0;
         cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
         cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
-        return freeB + (reserved > used ? size_t(reserved - used) : 0);
+        mLiveFree = freeB + (reserved > used ? size_t(reserved - used) : 0);
+        mLiveAt = now;
+        return mLiveFree;
     }
 
     // A batch of `bytes` is admitted while it fits what the batches in flight leave of the budget
@@ -289,8 +313,10 @@ private:
                 if (mPending.empty()) return false;
                 slot = freeSlot();
                 if (slot == nullptr) return false;
-                liveFree = liveFreeBytes();
-                return admits(estimate(mPending.front()->n, 1), liveFree);
+                const size_t bytes = estimate(mPending.front()->n, 1);
+                if (bytes + mReserved > mOpt.hbm_budget_bytes) return false;
+                liveFree = (mInflight.empty() && mReserved == 0) ? ~size_t(0) : liveFreeBytes();
+                return admits(bytes, liveFree);
             });
             if (mStop) {
                 for (auto& r : mPending) finishLocked(*r, RBW_ERR_INVALID_ARG, "server stopped");
@@ -312,6 +338,7 @@ private:
             }
             slot->reserved = estimate(desc, slot->reqs.size());
             mReserved += slot->reserved;
+            mLiveFree = mLiveFree > slot->reserved ? mLiveFree - slot->reserved : 0;
             slot->busy = true;
             mBatches++;
             mBatchedRequests += slot->reqs.size();
@@ -436,6 +463,8 @@ private:
     }
 
     PinnedPool mPinned; // destroyed after the threads (declared before them)
+    size_t mLiveFree = 0;
+    Clock::time_point mLiveAt{};
     const rbw_vocabulary* mVoc;
     rbw_database* mDb;
     rbw_server_options mOpt;
