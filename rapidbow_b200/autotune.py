@@ -8,6 +8,8 @@ tree levels, descriptor-count bucket = floor(log2(n))):
     assign_ctas_per_sm      uint8 k-means assign, CTAs per SM: 2..6         (default 6)
     assign_f32_ctas_per_sm  float-center assign, CTAs per SM: 1..3          (default 3)
     scatter_rows            lookup regroup scatter, rows per thread: 8|16|32 (default 16)
+    db_shard_tables         DataBase inverted file: 1 one CSR per 20,480-document shard while
+                            small, 2 one CSR (default 1; its bucket counts documents)
 
 Cache file (JSON): {"format": "rapidbow_b200 tuning cache", "version": 1,
 "device": {"name": ..., "sms": ...}, "entries": [{"param", "B", "L", "bucket", "value",
@@ -23,11 +25,14 @@ import os
 import re
 from typing import Callable, Dict, Iterable, List, Optional
 
+import numpy as np
+
 from . import _check, load_library
 
-PARAMS = {"assign_ctas_per_sm": 0, "assign_f32_ctas_per_sm": 1, "scatter_rows": 2}
-DEFAULTS = {"assign_ctas_per_sm": 6, "assign_f32_ctas_per_sm": 3, "scatter_rows": 16}
-CANDIDATES = {"assign_ctas_per_sm": (2, 3, 4, 5, 6), "assign_f32_ctas_per_sm": (1, 2, 3), "scatter_rows": (8, 16, 32)}
+PARAMS = {"assign_ctas_per_sm": 0, "assign_f32_ctas_per_sm": 1, "scatter_rows": 2, "db_shard_tables": 3}
+DEFAULTS = {"assign_ctas_per_sm": 6, "assign_f32_ctas_per_sm": 3, "scatter_rows": 16, "db_shard_tables": 1}
+CANDIDATES = {"assign_ctas_per_sm": (2, 3, 4, 5, 6), "assign_f32_ctas_per_sm": (1, 2, 3), "scatter_rows": (8, 16, 32),
+              "db_shard_tables": (1, 2)}
 FORMAT = "rapidbow_b200 tuning cache"
 VERSION = 1
 
@@ -182,3 +187,32 @@ class Autotuner:
             return timing_read("lookup_regroup")[0] / repeats
 
         return self.tune("scatter_rows", voc.branch_factor, voc.nb_levels, desc.shape[0], measure)
+
+    def tune_database(self, voc, doc_ids, leaves, offsets, query_leaves, query_offsets, max_results: int,
+                      repeats: int = 3) -> dict:
+        """Tunes the inverted-file layout (one CSR per document shard or one CSR) on batched queries
+        (CUDA uint32 leaves, uint64 offsets) against a database of the given documents (host
+        arrays, DataBase.add_docs form), timed by the library's scoring events.  The layout is
+        chosen when the index is built, so each candidate builds its own database."""
+        import torch
+
+        from . import timing_enable, timing_read, timing_reset
+        from .database import DataBase
+
+        n_docs = int(np.asarray(doc_ids).size)
+
+        def measure() -> float:
+            db = DataBase(voc)
+            db.add_docs(doc_ids, leaves, offsets)
+            db.query_batched(query_leaves, query_offsets, max_results)  # builds the index
+            torch.cuda.synchronize()
+            timing_reset()
+            timing_enable(True)
+            for _ in range(repeats):
+                db.query_batched(query_leaves, query_offsets, max_results)
+            torch.cuda.synchronize()
+            timing_enable(False)
+            del db
+            return timing_read("score")[0] / repeats
+
+        return self.tune("db_shard_tables", voc.branch_factor, voc.nb_levels, n_docs, measure)

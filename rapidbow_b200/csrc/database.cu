@@ -33,6 +33,7 @@
 #include "capi_internal.h"
 #include "kmeans.cuh"
 #include "timing.h"
+#include "tuning.h"
 
 #include <algorithm>
 #include <cmath>
@@ -50,6 +51,7 @@ constexpr uint32_t kPrepThreads = 512;
 constexpr uint32_t kScoreThreads = 1024;
 constexpr uint32_t kSegThreads = 256;
 constexpr uint32_t kSmemDocs = 20480;     // per-document accumulators kept in shared memory
+constexpr uint64_t kShardTableMinBytes = 64ull << 20; // per-shard CSR tables always allowed up to this size
 constexpr uint32_t kMaxK = 1024;          // results selected in shared memory; more in global memory
 constexpr double kFixScale = 72057594037927936.0; // 2^56
 constexpr uint32_t kDeltaMinDocs = 256;   // the delta may always hold this many documents
@@ -191,16 +193,25 @@ __global__ void __launch_bounds__(kPrepThreads) docPrepKernel(const uint32_t* ne
     if (threadIdx.x == 0) pairCount[slot] = cnt;
 }
 
-// Per-leaf pair and posting counts of the documents [s0, s0 + gridDim.x).
+// Row of a document's pairs in a segment's offset table: the per-shard CSR of its shard
+// (stride = leaves per shard table), or the single table (stride 0).
+__device__ __forceinline__ uint64_t segRow(uint32_t slot, uint32_t shardBeg, uint64_t stride)
+{
+    return stride ? uint64_t(slot / kSmemDocs - shardBeg) * stride : 0ull;
+}
+
+// Per-(shard, leaf) pair counts and per-leaf posting counts of the documents [s0, s0 + gridDim.x).
 __global__ void segCountKernel(const uint64_t* docOff, const uint64_t* docPairs, const uint32_t* pairCount,
-                               uint32_t s0, uint32_t* leafPairCnt, unsigned long long* leafPost)
+                               uint32_t s0, uint32_t shardBeg, uint64_t stride, uint32_t* leafPairCnt,
+                               unsigned long long* leafPost)
 {
     const uint32_t slot = s0 + blockIdx.x;
     const uint64_t beg = docOff[slot];
+    uint32_t* cnt = leafPairCnt + segRow(slot, shardBeg, stride);
     for (uint32_t p = threadIdx.x; p < pairCount[slot]; p += blockDim.x) {
         const uint64_t v = docPairs[beg + p];
         const uint32_t leaf = static_cast<uint32_t>(v >> 32);
-        atomicAdd(&leafPairCnt[leaf], 1u);
+        atomicAdd(&cnt[leaf], 1u);
         atomicAdd(&leafPost[leaf], static_cast<unsigned long long>(static_cast<uint32_t>(v)));
     }
 }
@@ -209,18 +220,20 @@ __global__ void segCountKernel(const uint64_t* docOff, const uint64_t* docPairs,
 // document entry d = tf * w_leaf * rcp (DataBase.cpp:129, the same float products as at query
 // time), tf[] = the raw count for the virtual inverted files of upper levels.
 __global__ void segScatterKernel(const uint64_t* docOff, const uint64_t* docPairs, const uint32_t* pairCount,
-                                 uint32_t s0, const float* leafWeights, const float* rcpF, const uint32_t* leafOff,
-                                 uint32_t* cursor, uint64_t* pairs, uint32_t* tfs)
+                                 uint32_t s0, uint32_t shardBeg, uint64_t stride, const float* leafWeights,
+                                 const float* rcpF, const uint32_t* leafOff, uint32_t* cursor, uint64_t* pairs,
+                                 uint32_t* tfs)
 {
     const uint32_t slot = s0 + blockIdx.x;
     const uint64_t beg = docOff[slot];
     const float rcp = rcpF[slot];
+    const uint64_t row = segRow(slot, shardBeg, stride);
     for (uint32_t p = threadIdx.x; p < pairCount[slot]; p += blockDim.x) {
         const uint64_t v = docPairs[beg + p];
         const uint32_t leaf = static_cast<uint32_t>(v >> 32);
         const uint32_t tf = static_cast<uint32_t>(v);
         const float d = float(tf) * leafWeights[leaf] * rcp;
-        const uint32_t pos = leafOff[leaf] + atomicAdd(&cursor[leaf], 1u);
+        const uint32_t pos = leafOff[row + leaf] + atomicAdd(&cursor[row + leaf], 1u);
         pairs[pos] = (uint64_t(slot) << 32) | __float_as_uint(d);
         tfs[pos] = tf;
     }
@@ -335,9 +348,11 @@ __global__ void __launch_bounds__(1024) workOrderKernel(const unsigned long long
 }
 
 struct SegmentView {
-    const uint32_t* leafOff;   // [nbLeaves + 1]
+    const uint32_t* leafOff;   // [nShards * stride + 1], or [nbLeaves + 1] when stride = 0
     const uint64_t* pairs;     // slot << 32 | float bits of the leaf-level document entry
     const uint32_t* tf;        // descriptors of the document under the leaf
+    uint64_t stride;           // nbLeaves: one CSR per shard of kSmemDocs slots; 0: one CSR
+    uint32_t shardBeg, nShards;
 };
 
 struct ScoreParams {
@@ -449,9 +464,10 @@ __device__ __forceinline__ void writeResults(const ScoreParams& P, uint32_t q, c
 }
 
 // One CTA per (query, shard of shardDocs documents).  The accumulators of the shard live in
-// shared memory (9 B per document); every CTA of a query walks all the query's postings and
-// keeps those of its shard.  kSharded = false: one shard holds every document and no posting
-// needs the shard test.
+// shared memory (9 B per document).  A segment indexed per shard hands each CTA the postings
+// of its own shard; a segment with one inverted file (stride 0) is walked by every CTA of the
+// query, each keeping the postings of its shard.  kSharded = false: one shard holds every
+// document and no posting needs the shard test.
 template <bool kSharded>
 __global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
 {
@@ -487,8 +503,15 @@ __global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
 #pragma unroll
         for (int s = 0; s < 2; s++) {
             const uint64_t* pairs = P.seg[s].pairs;
-            const uint32_t a = P.seg[s].leafOff[uint64_t(en.word) * span];
-            const uint32_t b = P.seg[s].leafOff[(uint64_t(en.word) + 1) * span];
+            const uint32_t* leafOff = P.seg[s].leafOff;
+            if (P.seg[s].stride) {
+                // this shard's own inverted file (none: the segment holds no document of it)
+                const uint32_t rel = shard - P.seg[s].shardBeg;
+                if (rel >= P.seg[s].nShards) continue;
+                leafOff += uint64_t(rel) * P.seg[s].stride;
+            }
+            const uint32_t a = leafOff[uint64_t(en.word) * span];
+            const uint32_t b = leafOff[(uint64_t(en.word) + 1) * span];
             if (leafLevel) {
                 // sixteen pairs per lane in flight
                 uint32_t p = a + lane;
@@ -634,10 +657,17 @@ private:
 };
 
 struct Segment {
-    PoolBuffer leafOff;   // u32 [nbLeaves + 1]
+    PoolBuffer leafOff;   // u32 [nShards * stride + 1]; [nbLeaves + 1] when stride = 0
     PoolBuffer pairs;     // u64 slot << 32 | float bits of the leaf-level document entry
     PoolBuffer tf;        // u32 per pair
     uint32_t slotBeg = 0, slotEnd = 0;
+    uint64_t stride = 0;  // nbLeaves when each shard of kSmemDocs slots has its own CSR
+    uint32_t shardBeg = 0, nShards = 1;
+    SegmentView view() const
+    {
+        return SegmentView{leafOff.as<uint32_t>(), pairs.as<uint64_t>(), tf.as<uint32_t>(), stride, shardBeg,
+                           nShards};
+    }
 };
 
 } // namespace
@@ -828,9 +858,8 @@ public:
             P.qOff = dOff;
             P.qRcpF = static_cast<const float*>(qr);
             P.weights = mWeights.as<float>();
-            P.seg[0] = SegmentView{mMain.leafOff.as<uint32_t>(), mMain.pairs.as<uint64_t>(), mMain.tf.as<uint32_t>()};
-            P.seg[1] = SegmentView{mDelta.leafOff.as<uint32_t>(), mDelta.pairs.as<uint64_t>(),
-                                   mDelta.tf.as<uint32_t>()};
+            P.seg[0] = mMain.view();
+            P.seg[1] = mDelta.view();
             P.rcpF = mRcpF.as<float>();
             P.slotDoc = mSlotDoc.as<uint32_t>();
             P.nDocs = nDocs;
@@ -946,9 +975,13 @@ public:
         updateIndex();
         std::shared_lock<std::shared_mutex> lk(mMu);
         std::vector<uint32_t> out;
-        for (const Segment* sg : {&mMain, &mDelta}) {
+        std::vector<std::pair<const Segment*, uint32_t>> tables; // (segment, shard table)
+        for (const Segment* sg : {&mMain, &mDelta})
+            for (uint32_t sh = 0; sh < sg->nShards; sh++) tables.emplace_back(sg, sh);
+        for (const auto& [sg, sh] : tables) {
             uint32_t ab[2] = {0, 0};
-            RBW_CUDA(cudaMemcpyAsync(ab, sg->leafOff.as<uint32_t>() + leaf, 8, cudaMemcpyDeviceToHost, mStream));
+            RBW_CUDA(cudaMemcpyAsync(ab, sg->leafOff.as<uint32_t>() + sh * sg->stride + leaf, 8,
+                                     cudaMemcpyDeviceToHost, mStream));
             RBW_CUDA(cudaStreamSynchronize(mStream));
             if (ab[1] < ab[0]) throw Error(kInternal, "inconsistent posting offsets");
             std::vector<uint64_t> pr(ab[1] - ab[0]);
@@ -1008,35 +1041,55 @@ private:
     }
 
     // CSR of the documents [s0, s1) into `sg`; their per-leaf posting counts into leafPost.
+    // Documents spanning several shards of kSmemDocs slots get one CSR per shard (each scoring
+    // CTA then reads only its shard's postings) while those tables stay small next to the
+    // postings themselves; otherwise one CSR that every CTA of a query filters.
     void buildSegment(Segment& sg, uint32_t s0, uint32_t s1, unsigned long long* leafPost)
     {
         const uint64_t pairsUpper = mHostDocOff[s1] - mHostDocOff[s0];
         if (pairsUpper >= 0xFFFFFFFFull) throw Error(kUnsupported, "more than 2^32 postings in one segment");
         sg.slotBeg = s0;
         sg.slotEnd = s1;
+        sg.stride = 0;
+        sg.shardBeg = 0;
+        sg.nShards = 1;
+        if (s1 > s0) {
+            const uint32_t first = s0 / kSmemDocs, last = (s1 - 1) / kSmemDocs;
+            const uint64_t tableBytes = (uint64_t(last - first + 1) * mNbLeaves + 1) * 4;
+            const bool allowed = tunedValue(kTuneDbShardTables, mB, mL, s1 - s0) == 1;
+            if (allowed && last > first &&
+                tableBytes <= std::max<uint64_t>(kShardTableMinBytes, pairsUpper * 12)) {
+                sg.stride = mNbLeaves;
+                sg.shardBeg = first;
+                sg.nShards = last - first + 1;
+            }
+        }
+        const uint64_t entries = uint64_t(sg.nShards) * mNbLeaves;
+        sg.leafOff.reserve((entries + 1) * 4, 0, mStream);
         sg.pairs.reserve(std::max<uint64_t>(pairsUpper, 1) * 8, 0, mStream);
         sg.tf.reserve(std::max<uint64_t>(pairsUpper, 1) * 4, 0, mStream);
         void* tmp = nullptr;
-        const size_t cntBytes = mNbLeaves * 4;
-        const size_t scanBytes = scanTempWords(mNbLeaves) * 4;
+        const size_t cntBytes = entries * 4;
+        const size_t scanBytes = scanTempWords(entries) * 4;
         RBW_CUDA(cudaMallocFromPoolAsync(&tmp, 2 * cntBytes + scanBytes, libraryPool(), mStream));
         uint32_t* leafPairCnt = static_cast<uint32_t*>(tmp);
-        uint32_t* cursor = leafPairCnt + mNbLeaves;
-        uint32_t* scanTmp = cursor + mNbLeaves;
+        uint32_t* cursor = leafPairCnt + entries;
+        uint32_t* scanTmp = cursor + entries;
         RBW_CUDA(cudaMemsetAsync(leafPairCnt, 0, 2 * cntBytes, mStream));
         RBW_CUDA(cudaMemsetAsync(leafPost, 0, mNbLeaves * 8, mStream));
         if (s1 > s0) {
             segCountKernel<<<s1 - s0, kSegThreads, 0, mStream>>>(mDocOff.as<uint64_t>(), mDocPairs.as<uint64_t>(),
-                                                                mPairCount.as<uint32_t>(), s0, leafPairCnt, leafPost);
+                                                                mPairCount.as<uint32_t>(), s0, sg.shardBeg,
+                                                                sg.stride, leafPairCnt, leafPost);
             RBW_CUDA(cudaGetLastError());
         }
         uint32_t* leafOff = sg.leafOff.as<uint32_t>();
-        exclusiveScanU32(leafPairCnt, leafOff, mNbLeaves, scanTmp, mStream);
-        leafOffTail<<<1, 1, 0, mStream>>>(leafPairCnt, leafOff, mNbLeaves);
+        exclusiveScanU32(leafPairCnt, leafOff, entries, scanTmp, mStream);
+        leafOffTail<<<1, 1, 0, mStream>>>(leafPairCnt, leafOff, entries);
         if (s1 > s0) {
             segScatterKernel<<<s1 - s0, kSegThreads, 0, mStream>>>(
-                mDocOff.as<uint64_t>(), mDocPairs.as<uint64_t>(), mPairCount.as<uint32_t>(), s0,
-                mWeights.as<float>() + levelBeg(mB, mL - 1) * mB, mRcpF.as<float>(), leafOff, cursor,
+                mDocOff.as<uint64_t>(), mDocPairs.as<uint64_t>(), mPairCount.as<uint32_t>(), s0, sg.shardBeg,
+                sg.stride, mWeights.as<float>() + levelBeg(mB, mL - 1) * mB, mRcpF.as<float>(), leafOff, cursor,
                 sg.pairs.as<uint64_t>(), sg.tf.as<uint32_t>());
         }
         RBW_CUDA(cudaGetLastError());

@@ -18,6 +18,7 @@ bool valid(TuneParam p, uint32_t v)
     case kTuneAssignCtasPerSm: return v >= 1 && v <= 6;
     case kTuneAssignFCtasPerSm: return v >= 1 && v <= 3;
     case kTuneScatterRows: return v == 8 || v == 16 || v == 32;
+    case kTuneDbShardTables: return v == 1 || v == 2;
     default: return false;
     }
 }
@@ -40,6 +41,7 @@ uint32_t tuneDefault(TuneParam p)
     case kTuneAssignCtasPerSm: return 6;
     case kTuneAssignFCtasPerSm: return 3;
     case kTuneScatterRows: return 16;
+    case kTuneDbShardTables: return 1;
     default: return 0;
     }
 }

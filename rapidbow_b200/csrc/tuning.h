@@ -10,7 +10,8 @@ enum TuneParam : uint32_t {
     kTuneAssignCtasPerSm = 0,  // uint8 k-means assign: resident CTAs per SM, 1..6 (default 6)
     kTuneAssignFCtasPerSm = 1, // float-center assign: resident CTAs per SM, 1..3 (default 3)
     kTuneScatterRows = 2,      // lookup regroup scatter: rows per thread, 8 | 16 | 32 (default 16)
-    kTuneParamCount = 3,
+    kTuneDbShardTables = 3,    // inverted file: 1 one CSR per shard while small (default), 2 one CSR
+    kTuneParamCount = 4,
 };
 
 // floor(log2(max(n, 1))): workloads within a factor of two share an entry.

@@ -231,6 +231,51 @@ def test_many_documents_use_global_accumulators(oracle):
         check_query(db, odb, np.concatenate([q, np.arange(0, B ** L, 7, dtype=np.uint32)]), 1500)
 
 
+@pytest.mark.parametrize("layout", [1, 2])
+def test_shard_tables_and_single_table_match_oracle(oracle, layout):
+    """Both inverted-file layouts (one CSR per 20,480-document shard, one CSR for the segment),
+    with a main segment over two shards and a delta segment that straddles a shard boundary;
+    results, postings and upper-level (virtual) inverted files match the oracle."""
+    from rapidbow_b200 import autotune as at
+
+    B, L = 16, 3
+    n_main, n_delta = 39000, 3000
+    docs = make_docs(n_main + n_delta, B ** L, seed=41, lo=2, hi=30, zipf=1.0)
+    centers, masks, weights = random_tree(B, L, 42, dup_rate=0.0)
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    at.clear()
+    try:
+        for bkt in range(32):
+            at.set_value("db_shard_tables", B, L, bkt, layout)
+        db = rbw.DataBase(voc)
+        odb = oracle.db(B, L, weights)
+
+        def add(lo, hi):
+            offs = np.zeros(hi - lo + 1, np.uint64)
+            offs[1:] = np.cumsum([d.size for d in docs[lo:hi]])
+            db.add_docs(np.arange(lo, hi, dtype=np.uint32), np.concatenate(docs[lo:hi]), offs)
+            for i in range(lo, hi):
+                odb.add(i, docs[i])
+
+        add(0, n_main)
+        qs = make_queries(docs[:n_main], B ** L, 6, seed=43)
+        # a query of rare leaves: upper-level words pass the skip rule
+        qs.append(np.concatenate([docs[n_main - 1], docs[5], docs[30000]]))
+        for q in qs:
+            check_query(db, odb, q, 40)
+        assert db.segments() == (n_main, 0)
+        add(n_main, n_main + n_delta)  # slots 39000..41999: shards 1 and 2
+        qs.append(np.concatenate([docs[n_main + 2999], docs[40960]]))
+        for q in qs:
+            check_query(db, odb, q, 40)
+        check_query(db, odb, np.concatenate([qs[0], np.arange(0, B ** L, 5, dtype=np.uint32)]), 1200)
+        assert db.segments() == (n_main, n_delta)
+        for leaf in {int(docs[0][0]), int(docs[20480][0]), int(docs[n_main + 1500][0]), int(docs[41999][-1])}:
+            assert np.array_equal(db.postings(leaf), odb.postings(leaf))
+    finally:
+        at.clear()
+
+
 def test_large_documents_queries_and_result_sets(oracle):
     """Documents and queries above 32,768 descriptors (sorted in global memory) and k = 2,000
     (selected in global memory) against the oracle, single and batched; the reference's
