@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--n", type=int, default=N_LOOKUP)
-    p.add_argument("--algo", default="auto", choices=["auto", "tensor_u8", "tensor_u8_warpnode"],
+    p.add_argument("--algo", default="auto", choices=["auto", "tensor_u8", "tensor_u8_warpnode", "tensor_u8_ring"],
                    help="tensor-core lookup variant of the timed steps (auto = the library's default)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     p.add_argument("--no-cpu-baseline", action="store_true")

@@ -92,8 +92,10 @@ enum {
     RBW_LOOKUP_AUTO = 0,       /* fastest exact path */
     RBW_LOOKUP_TENSOR_U8 = 1,  /* tcgen05 uint8 tensor-core descent with device regroup */
     RBW_LOOKUP_SIMT_F32 = 2,   /* plain FP32 SIMT descent (comparison baseline) */
-    RBW_LOOKUP_TENSOR_U8_WARPNODE = 3 /* as TENSOR_U8, the node level of each level pair by warp-level MMAs
-                                         in the epilogue warps, so the children MMA need not wait for it */
+    RBW_LOOKUP_TENSOR_U8_WARPNODE = 3, /* as TENSOR_U8, the node level of each level pair by warp-level MMAs
+                                          in the epilogue warps, so the children MMA need not wait for it */
+    RBW_LOOKUP_TENSOR_U8_RING = 4      /* as TENSOR_U8, the node level and the children (in halves) in
+                                          separate tensor-memory columns: one issuer, a three-slot ring */
 };
 
 RBW_API const char* rbw_last_error(void);

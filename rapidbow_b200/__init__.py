@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(HERE, "lib", "librapidbow_b200.so")
 
 RBW_OK, RBW_ERR_INVALID_ARG, RBW_ERR_UNSUPPORTED, RBW_ERR_OUT_OF_MEMORY, RBW_ERR_CUDA, RBW_ERR_TIMEOUT, \
     RBW_ERR_INVALID_BLOB, RBW_ERR_DUPLICATE, RBW_ERR_INTERNAL = range(9)
-LOOKUP_ALGOS = {"auto": 0, "tensor_u8": 1, "simt_f32": 2, "tensor_u8_warpnode": 3}
+LOOKUP_ALGOS = {"auto": 0, "tensor_u8": 1, "simt_f32": 2, "tensor_u8_warpnode": 3, "tensor_u8_ring": 4}
 INIT_MODES = {"reference": 0, "kmeans++": 1, "injected": 2}
 DATA_BINARY, DATA_UINT8 = 0, 1
 DIST_HAMMING, DIST_L1, DIST_L2 = 0, 1, 2

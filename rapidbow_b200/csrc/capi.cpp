@@ -172,7 +172,7 @@ int rbw_voc_lookup_ex(const rbw_vocabulary* voc, const void* dev_desc, uint64_t 
                       int32_t algo, void* stream, uint32_t* kernels_launched)
 {
     return guard([&] {
-        if (algo < 0 || algo > rbw::kLookupTensorU8WarpNode)
+        if (algo < 0 || algo > rbw::kLookupAlgoLast)
             throw rbw::Error(rbw::kInvalidArg, "unknown lookup algorithm");
         const uint32_t k = vocOf(voc).lookup(static_cast<const uint8_t*>(dev_desc), nb_desc, dev_leaf,
                                              static_cast<rbw::LookupAlgo>(algo), static_cast<cudaStream_t>(stream));
@@ -184,7 +184,7 @@ int rbw_voc_lookup_host(const rbw_vocabulary* voc, const void* host_desc, uint64
                         int32_t algo, uint32_t* kernels_launched)
 {
     return guard([&] {
-        if (algo < 0 || algo > rbw::kLookupTensorU8WarpNode)
+        if (algo < 0 || algo > rbw::kLookupAlgoLast)
             throw rbw::Error(rbw::kInvalidArg, "unknown lookup algorithm");
         const uint32_t k = rbw::lookupHostPipelined(vocOf(voc), static_cast<const uint8_t*>(host_desc), nb_desc,
                                                     host_leaf, static_cast<rbw::LookupAlgo>(algo));

@@ -39,12 +39,20 @@ constexpr uint32_t kTeamWarps = 4;                    // epilogue team: one warp
 constexpr uint32_t kIssuer1Warp = 2 + 2 * kTeamWarps;        // second MMA issuer, after the teams
 constexpr uint32_t kTcThreads = 32 * (3 + 2 * kTeamWarps); // TMA, two MMA issuers, two epilogue teams
 constexpr uint32_t kSmemHistMax = 1024;
+constexpr uint32_t kRegroupCtas = 296;                // regroup kernels' CTAs (2 per SM on 148 SMs)
 // Two accumulator buffers of 256 columns; tile t uses buffer t & 1.  Its level-2p MMA (16
 // columns) lands in the first columns of the buffer and is read by the buffer's epilogue team
 // before the children MMA of the same tile overwrites the buffer.
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kTmemBuf = 256;
 constexpr uint32_t kTileCache = 1024;
+// Ring schedule: three 128-column slots for the children accumulators (a tile's children in one
+// or two halves of at most 8 children) and eight 16-column node-level entries after them.
+constexpr uint32_t kRingSlots = 3;
+constexpr uint32_t kSlotCols = 128;
+constexpr uint32_t kNodeEntries = 8;
+constexpr uint32_t kNodeCol0 = kRingSlots * kSlotCols;
+static_assert(kNodeCol0 + 16 * kNodeEntries <= kTmemCols, "ring schedule exceeds tensor memory");
 constexpr uint32_t kGatherDepth = 4;                  // gathered tiles in flight (< kStages)
 // Row-index ring: iteration i reads slot i % kIdxSlots and queues the copy of tile i + kGatherDepth
 // into slot (i + kGatherDepth) % kIdxSlots, which was last read in iteration i - 1 (behind that
@@ -65,6 +73,11 @@ struct TcSmem {
     uint64_t bufFree[2];  // the last reader of buffer j is done with it
     uint64_t lowFree[2];  // team j has read columns [0, 128) of buffer j (two levels only)
     uint64_t mmaDone;
+    // ring schedule (lookupPassRing)
+    uint64_t nodeAcc[8];  // node-level MMA of tile t complete (entry t % kNodeEntries)
+    uint64_t nodeFree[8]; // the team has read entry t % kNodeEntries
+    uint64_t slotFull[3]; // children MMA of half n complete (slot n % kRingSlots)
+    uint64_t slotFree[3]; // the team has read slot n % kRingSlots
     uint32_t tmemBase;
     uint32_t abortFlag;
     alignas(16) int32_t cn[2][17][16]; // |c|^2 of each B slot: row 0 = node, rows 1.. = children
@@ -88,7 +101,7 @@ struct PassParams {
     const uint32_t* nTilesDev;
     uint32_t* out;           // final pass: leaf index per descriptor
     uint32_t* nodeNext;      // other passes: in-level node index at level 2p + 2
-    uint32_t* binCount;      // other passes: histogram of nodeNext
+    uint32_t* binCount;      // other passes: histogram of nodeNext (nullptr: counted by regroupHist)
     uint32_t nbBins;
     uint32_t isFinal;
     DeviceErrors* err;
@@ -263,10 +276,143 @@ __device__ __forceinline__ void emitRow(TcSmem& S, const PassParams& p, bool sme
         p.nodeNext[orig] = node;
         if (smemHist) {
             atomicAdd(&S.hist[node], 1u);
-        } else {
+        } else if (p.binCount != nullptr) {
             atomicAdd(&p.binCount[node], 1u);
         }
     }
+}
+
+// ------------------------------------------------------------------ producer warp
+// Stages the CTA's tiles [t0, t0 + nT) into the kStages shared-memory slots (arrival on aFull[s],
+// waits on aEmpty[s]) and each centre group's block (node + children, bFull / bEmpty).
+__device__ __forceinline__ void passProducer(TcSmem& S, const PassParams& p, const CUtensorMap* tmapTile,
+                                             uint32_t t0, uint32_t nT, uint32_t lane, volatile uint32_t* abortFlag)
+{
+    const bool two = p.twoLevels != 0;
+    const bool gather = p.perm != nullptr;
+    // First pass: one TMA tiled load (128 rows, 128-byte swizzle) per tile.
+    // Later passes: the tile's 128 rows are gathered with 16-byte cp.async (lane q copies chunk
+    // q % 8 of rows 32 (q / 8) + k) into the same swizzled layout, kGatherDepth tiles in flight.
+    // Row indices travel through a shared-memory ring inside the same copy groups: group #i
+    // (prologue for i < kGatherDepth, else committed by iteration i - kGatherDepth) carries
+    // the indices of tile i and the rows of tile i - kGatherDepth, so wait_group(depth - 1)
+    // at the top of iteration i completes both; those rows are then published to the MMA
+    // with a proxy fence (generic-proxy writes, async-proxy reader) and an arrival.
+    auto copyIdx = [&](uint32_t i) {
+        if (i < nT) {
+            const TileInfo ti = tileAtSmem(S, p, t0, i);
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+                const uint32_t rr = 4 * lane + j;
+                cpAsync4(&S.idx[i % kIdxSlots][rr], p.perm + ti.start + (rr < ti.count ? rr : 0u));
+            }
+        }
+    };
+    uint32_t published = 0; // tiles [0, published) are visible to the MMA
+    auto publishUpTo = [&](uint32_t end) {
+        if (published >= end) return;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0)
+            for (uint32_t j = published; j < end; j++) mbarArrive(&S.aFull[j % kStages]);
+        published = end;
+    };
+    if (gather) {
+        for (uint32_t d = 0; d < kGatherDepth; d++) {
+            copyIdx(d);
+            cpAsyncCommit();
+        }
+    }
+    uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, slotUses0 = 0, slotUses1 = 0;
+    uint32_t issued = 0;
+    for (uint32_t i = 0; i < nT; i++) {
+        const TileInfo ti = tileAtSmem(S, p, t0, i);
+        if (gather) {
+            cpAsyncWait<kGatherDepth - 1>();
+            if (i >= kGatherDepth) publishUpTo(i - kGatherDepth + 1);
+        }
+        bool ok = true;
+        if (ti.group != prevGroup) {
+            // A slot is released only after the MMA and epilogue are done with tile i-2 or
+            // earlier, so every gathered tile must be published before waiting for it.
+            if (gather) {
+                cpAsyncWait<0>();
+                publishUpTo(i);
+            }
+            slot ^= 1u;
+            const uint32_t k = slot ? slotUses1++ : slotUses0++;
+            if (lane == 0) {
+                ok = mbarWait(&S.bEmpty[slot], (k & 1u) ^ 1u, abortFlag, p.err, 10);
+                if (ok) {
+                    const uint32_t nb = two ? p.B : 0u;
+                    mbarArriveExpectTx(&S.bFull[slot], (kNodeBytes + 64u) * (1u + nb));
+                    bulkLoad(S.b[slot], p.centersSw + (p.lbA + ti.group) * kNodeBytes, kNodeBytes, &S.bFull[slot]);
+                    bulkLoad(&S.cn[slot][0][0], p.cnorm + (p.lbA + ti.group) * kMaxBranch, 64u, &S.bFull[slot]);
+                    if (two) {
+                        const uint64_t c0 = p.lbB + uint64_t(ti.group) * p.B;
+                        bulkLoad(S.b[slot] + kNodeBytes, p.centersSw + c0 * kNodeBytes, kNodeBytes * p.B,
+                                 &S.bFull[slot]);
+                        bulkLoad(&S.cn[slot][1][0], p.cnorm + c0 * kMaxBranch, 64u * p.B, &S.bFull[slot]);
+                    }
+                }
+            }
+            ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+            if (!ok) break;
+            prevGroup = ti.group;
+        }
+        const uint32_t s = i % kStages;
+        const uint32_t ph = (i / kStages) & 1u;
+        if (lane == 0) {
+            ok = mbarWait(&S.aEmpty[s], ph ^ 1u, abortFlag, p.err, 11);
+            if (ok && !gather) mbarArriveExpectTx(&S.aFull[s], kTileBytes);
+        }
+        ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+        if (!ok) break;
+        if (!gather) {
+            if (lane == 0) tmaLoad2d(S.a[s], tmapTile, 0, static_cast<int32_t>(ti.start), &S.aFull[s]);
+        } else {
+            // Eight consecutive lanes copy the eight 16-byte chunks of one row, so each
+            // instruction moves four whole 128-byte rows (4 lines, not 32).  The indices were
+            // written by other lanes' copies: the wait above plus this barrier make them visible.
+            __syncwarp();
+            // All indices are read before the first copy: the copies are ordered with shared
+            // memory accesses, so reads interleaved with them would each wait in turn.
+            // Lane group g = lane / 8 copies rows 32 g .. 32 g + 31, whose indices it reads
+            // with eight 16-byte loads.
+            const int32_t* ring = &S.idx[i % kIdxSlots][0];
+            const uint32_t c = lane & 7u;
+            uint32_t rowIdx[kTileRows / 4];
+#pragma unroll
+            for (uint32_t k = 0; k < kTileRows / 16; k++) {
+                const int4 v = *reinterpret_cast<const int4*>(ring + 32u * (lane >> 3) + 4u * k);
+                rowIdx[4 * k] = static_cast<uint32_t>(v.x);
+                rowIdx[4 * k + 1] = static_cast<uint32_t>(v.y);
+                rowIdx[4 * k + 2] = static_cast<uint32_t>(v.z);
+                rowIdx[4 * k + 3] = static_cast<uint32_t>(v.w);
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kTileRows / 4; k++) {
+                const uint32_t tr = 32u * (lane >> 3) + k; // row within the tile
+                cpAsync16(S.a[s] + tr * kDims + ((c ^ (tr & 7u)) << 4), p.desc + uint64_t(rowIdx[k]) * kDims + (c << 4));
+            }
+            copyIdx(i + kGatherDepth);
+            cpAsyncCommit();
+        }
+        issued = i + 1;
+        __syncwarp();
+    }
+    if (gather) {
+        cpAsyncWait<0>();
+        publishUpTo(issued);
+    } else if (lane == 0) {
+        // Drain: every TMA load this warp issued must land before the CTA can exit.
+        const uint32_t armed = issued < kStages ? issued : kStages;
+        for (uint32_t s = 0; s < armed; s++) {
+            const uint32_t last = ((issued - 1 - s) / kStages) * kStages + s; // last i with i % kStages == s
+            mbarWait(&S.aFull[s], (last / kStages) & 1u, abortFlag, p.err, 12);
+        }
+    }
+    __syncwarp();
 }
 
 // kWarpNode = false: both levels on tcgen05, the node-level MMA and the children MMA of a tile in
@@ -288,7 +434,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t t0 = static_cast<uint32_t>(uint64_t(T) * blockIdx.x / gridDim.x);
     const uint32_t t1 = static_cast<uint32_t>(uint64_t(T) * (blockIdx.x + 1) / gridDim.x);
     const uint32_t nT = t1 - t0;
-    const bool smemHist = !p.isFinal && p.nbBins <= kSmemHistMax;
+    const bool smemHist = !p.isFinal && p.binCount != nullptr && p.nbBins <= kSmemHistMax;
     const bool two = p.twoLevels != 0;
     const bool gather = p.perm != nullptr;
     volatile uint32_t* abortFlag = &S.abortFlag;
@@ -328,130 +474,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tcFenceAfter();
     const uint32_t tmem = S.tmemBase;
     if (nT > 0 && warp == 0) {
-        // ------------------------------------------------------------ producer
-        // First pass: one TMA tiled load (128 rows, 128-byte swizzle) per tile.
-        // Later passes: the tile's 128 rows are gathered with 16-byte cp.async (lane q copies chunk
-        // q % 8 of rows 32 (q / 8) + k) into the same swizzled layout, kGatherDepth tiles in flight.
-        // Row indices travel through a shared-memory ring inside the same copy groups: group #i
-        // (prologue for i < kGatherDepth, else committed by iteration i - kGatherDepth) carries
-        // the indices of tile i and the rows of tile i - kGatherDepth, so wait_group(depth - 1)
-        // at the top of iteration i completes both; those rows are then published to the MMA
-        // with a proxy fence (generic-proxy writes, async-proxy reader) and an arrival.
-        auto copyIdx = [&](uint32_t i) {
-            if (i < nT) {
-                const TileInfo ti = tileAtSmem(S, p, t0, i);
-#pragma unroll
-                for (uint32_t j = 0; j < 4; j++) {
-                    const uint32_t rr = 4 * lane + j;
-                    cpAsync4(&S.idx[i % kIdxSlots][rr], p.perm + ti.start + (rr < ti.count ? rr : 0u));
-                }
-            }
-        };
-        uint32_t published = 0; // tiles [0, published) are visible to the MMA
-        auto publishUpTo = [&](uint32_t end) {
-            if (published >= end) return;
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncwarp();
-            if (lane == 0)
-                for (uint32_t j = published; j < end; j++) mbarArrive(&S.aFull[j % kStages]);
-            published = end;
-        };
-        if (gather) {
-            for (uint32_t d = 0; d < kGatherDepth; d++) {
-                copyIdx(d);
-                cpAsyncCommit();
-            }
-        }
-        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, slotUses0 = 0, slotUses1 = 0;
-        uint32_t issued = 0;
-        for (uint32_t i = 0; i < nT; i++) {
-            const TileInfo ti = tileAtSmem(S, p, t0, i);
-            if (gather) {
-                cpAsyncWait<kGatherDepth - 1>();
-                if (i >= kGatherDepth) publishUpTo(i - kGatherDepth + 1);
-            }
-            bool ok = true;
-            if (ti.group != prevGroup) {
-                // A slot is released only after the MMA and epilogue are done with tile i-2 or
-                // earlier, so every gathered tile must be published before waiting for it.
-                if (gather) {
-                    cpAsyncWait<0>();
-                    publishUpTo(i);
-                }
-                slot ^= 1u;
-                const uint32_t k = slot ? slotUses1++ : slotUses0++;
-                if (lane == 0) {
-                    ok = mbarWait(&S.bEmpty[slot], (k & 1u) ^ 1u, abortFlag, p.err, 10);
-                    if (ok) {
-                        const uint32_t nb = two ? p.B : 0u;
-                        mbarArriveExpectTx(&S.bFull[slot], (kNodeBytes + 64u) * (1u + nb));
-                        bulkLoad(S.b[slot], p.centersSw + (p.lbA + ti.group) * kNodeBytes, kNodeBytes, &S.bFull[slot]);
-                        bulkLoad(&S.cn[slot][0][0], p.cnorm + (p.lbA + ti.group) * kMaxBranch, 64u, &S.bFull[slot]);
-                        if (two) {
-                            const uint64_t c0 = p.lbB + uint64_t(ti.group) * p.B;
-                            bulkLoad(S.b[slot] + kNodeBytes, p.centersSw + c0 * kNodeBytes, kNodeBytes * p.B,
-                                     &S.bFull[slot]);
-                            bulkLoad(&S.cn[slot][1][0], p.cnorm + c0 * kMaxBranch, 64u * p.B, &S.bFull[slot]);
-                        }
-                    }
-                }
-                ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
-                if (!ok) break;
-                prevGroup = ti.group;
-            }
-            const uint32_t s = i % kStages;
-            const uint32_t ph = (i / kStages) & 1u;
-            if (lane == 0) {
-                ok = mbarWait(&S.aEmpty[s], ph ^ 1u, abortFlag, p.err, 11);
-                if (ok && !gather) mbarArriveExpectTx(&S.aFull[s], kTileBytes);
-            }
-            ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
-            if (!ok) break;
-            if (!gather) {
-                if (lane == 0) tmaLoad2d(S.a[s], &tmapTile, 0, static_cast<int32_t>(ti.start), &S.aFull[s]);
-            } else {
-                // Eight consecutive lanes copy the eight 16-byte chunks of one row, so each
-                // instruction moves four whole 128-byte rows (4 lines, not 32).  The indices were
-                // written by other lanes' copies: the wait above plus this barrier make them visible.
-                __syncwarp();
-                // All indices are read before the first copy: the copies are ordered with shared
-                // memory accesses, so reads interleaved with them would each wait in turn.
-                // Lane group g = lane / 8 copies rows 32 g .. 32 g + 31, whose indices it reads
-                // with eight 16-byte loads.
-                const int32_t* ring = &S.idx[i % kIdxSlots][0];
-                const uint32_t c = lane & 7u;
-                uint32_t rowIdx[kTileRows / 4];
-#pragma unroll
-                for (uint32_t k = 0; k < kTileRows / 16; k++) {
-                    const int4 v = *reinterpret_cast<const int4*>(ring + 32u * (lane >> 3) + 4u * k);
-                    rowIdx[4 * k] = static_cast<uint32_t>(v.x);
-                    rowIdx[4 * k + 1] = static_cast<uint32_t>(v.y);
-                    rowIdx[4 * k + 2] = static_cast<uint32_t>(v.z);
-                    rowIdx[4 * k + 3] = static_cast<uint32_t>(v.w);
-                }
-#pragma unroll
-                for (uint32_t k = 0; k < kTileRows / 4; k++) {
-                    const uint32_t tr = 32u * (lane >> 3) + k; // row within the tile
-                    cpAsync16(S.a[s] + tr * kDims + ((c ^ (tr & 7u)) << 4), p.desc + uint64_t(rowIdx[k]) * kDims + (c << 4));
-                }
-                copyIdx(i + kGatherDepth);
-                cpAsyncCommit();
-            }
-            issued = i + 1;
-            __syncwarp();
-        }
-        if (gather) {
-            cpAsyncWait<0>();
-            publishUpTo(issued);
-        } else if (lane == 0) {
-            // Drain: every TMA load this warp issued must land before the CTA can exit.
-            const uint32_t armed = issued < kStages ? issued : kStages;
-            for (uint32_t s = 0; s < armed; s++) {
-                const uint32_t last = ((issued - 1 - s) / kStages) * kStages + s; // last i with i % kStages == s
-                mbarWait(&S.aFull[s], (last / kStages) & 1u, abortFlag, p.err, 12);
-            }
-        }
-        __syncwarp();
+        passProducer(S, p, &tmapTile, t0, nT, lane, abortFlag);
     } else if (nT > 0 && (warp == 1 || warp == kIssuer1Warp)) {
         // ------------------------------------------------------------ MMA issuers (one thread each)
         // Issuer j (warp 1 for j = 0, warp kIssuer1Warp for j = 1) issues the MMAs of the tiles
@@ -646,6 +669,219 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
 }
 
+// Ring schedule.  One thread issues every MMA in tile order: the node-level MMA of tile t into
+// node entry t % kNodeEntries, then the tile's children in halves (children [0, c0) and
+// [c0, B), c0 = ceil(B / 2), one half when B <= 8) into ring slots n % kRingSlots, n = the
+// running half index.  No children MMA waits for a node-level read: the children accumulators
+// never share columns with the node level, so the tensor pipe runs the halves back to back
+// while the teams read earlier slots.  Half n waits only until half n - kRingSlots has been
+// read; node entry t until tile t - kNodeEntries's entry has been read.  Team t & 1 reads the
+// node level, picks the branch b, then reads the halves (64-column loads) and keeps the 16
+// columns of child b.
+__global__ void __launch_bounds__(kTcThreads, 1)
+    lookupPassRing(const __grid_constant__ CUtensorMap tmapTile, const PassParams p)
+{
+    extern __shared__ uint8_t smemRaw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+    const uint32_t warp = threadIdx.x / 32;
+    const uint32_t lane = threadIdx.x % 32;
+    const uint32_t T = p.tiles == nullptr ? static_cast<uint32_t>((p.nRows + kTileRows - 1) / kTileRows)
+                                          : *p.nTilesDev;
+    const uint32_t t0 = static_cast<uint32_t>(uint64_t(T) * blockIdx.x / gridDim.x);
+    const uint32_t t1 = static_cast<uint32_t>(uint64_t(T) * (blockIdx.x + 1) / gridDim.x);
+    const uint32_t nT = t1 - t0;
+    const bool smemHist = !p.isFinal && p.binCount != nullptr && p.nbBins <= kSmemHistMax;
+    const bool two = p.twoLevels != 0;
+    const uint32_t nh = two ? (p.B > 8 ? 2u : 1u) : 0u;   // children halves per tile
+    const uint32_t c0 = nh == 2 ? (p.B + 1) / 2 : p.B;     // children in the first half
+    volatile uint32_t* abortFlag = &S.abortFlag;
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < kStages; s++) {
+            mbarInit(&S.aFull[s], 1);
+            mbarInit(&S.aEmpty[s], 1);
+        }
+        for (uint32_t j = 0; j < 2; j++) {
+            mbarInit(&S.bFull[j], 1);
+            mbarInit(&S.bEmpty[j], 1 + 2 * kTeamWarps); // the issuer + both epilogue teams
+        }
+        for (uint32_t e = 0; e < kNodeEntries; e++) {
+            mbarInit(&S.nodeAcc[e], 1);
+            mbarInit(&S.nodeFree[e], kTeamWarps);
+        }
+        for (uint32_t k = 0; k < kRingSlots; k++) {
+            mbarInit(&S.slotFull[k], 1);
+            mbarInit(&S.slotFree[k], kTeamWarps);
+        }
+        mbarInit(&S.mmaDone, 1);
+        S.abortFlag = 0;
+        fenceMbarInit();
+    }
+    if (smemHist) {
+        for (uint32_t i = threadIdx.x; i < p.nbBins; i += blockDim.x) S.hist[i] = 0;
+    }
+    if (p.tiles != nullptr) {
+        const uint32_t m = nT < kTileCache ? nT : kTileCache;
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) S.tileCache[i] = p.tiles[t0 + i];
+    }
+    if (warp == 0) {
+        tmemAlloc(&S.tmemBase, kTmemCols);
+        tmemRelinquish();
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tmem = S.tmemBase;
+    if (nT > 0 && warp == 0) {
+        passProducer(S, p, &tmapTile, t0, nT, lane, abortFlag);
+    } else if (nT > 0 && warp == 1) {
+        // ------------------------------------------------------------ MMA issuer (one thread)
+        if (lane == 0) {
+            const uint32_t idescNode = idescU8(16);
+            uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, uses0 = 0, uses1 = 0;
+            bool ok = true;
+            for (uint32_t t = 0; ok && t < nT; t++) {
+                const TileInfo ti = tileAtSmem(S, p, t0, t);
+                if (ti.group != prevGroup) {
+                    slot ^= 1u;
+                    const uint32_t u = slot ? uses1++ : uses0++;
+                    if (!mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 40)) break;
+                    prevGroup = ti.group;
+                }
+                const uint32_t s = t % kStages;
+                if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 41)) break;
+                const uint32_t e = t % kNodeEntries;
+                if (t >= kNodeEntries && !mbarWait(&S.nodeFree[e], ((t / kNodeEntries) - 1u) & 1u, abortFlag, p.err, 42))
+                    break;
+                tcFenceAfter();
+                const uint32_t aBase = smemAddr(S.a[s]);
+                const uint32_t bBase = smemAddr(S.b[slot]);
+#pragma unroll
+                for (uint32_t q4 = 0; q4 < 4; q4++) {
+                    mmaU8(tmem + kNodeCol0 + 16u * e, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4),
+                          idescNode, q4 > 0 ? 1u : 0u);
+                }
+                mmaCommit(&S.nodeAcc[e]);
+                for (uint32_t h = 0; h < nh; h++) {
+                    const uint32_t n = t * nh + h;
+                    const uint32_t k = n % kRingSlots;
+                    if (n >= kRingSlots && !mbarWait(&S.slotFree[k], ((n / kRingSlots) - 1u) & 1u, abortFlag, p.err, 43)) {
+                        ok = false;
+                        break;
+                    }
+                    tcFenceAfter();
+                    const uint32_t cb = h ? c0 : 0u;
+                    const uint32_t cnt = h ? p.B - c0 : c0;
+                    const uint32_t idesc = idescU8(16u * cnt);
+                    const uint32_t cBase = bBase + kNodeBytes * (1u + cb);
+#pragma unroll
+                    for (uint32_t q4 = 0; q4 < 4; q4++) {
+                        mmaU8(tmem + kSlotCols * k, smemDescSw128(aBase + 32u * q4), smemDescSw128(cBase + 32u * q4),
+                              idesc, q4 > 0 ? 1u : 0u);
+                    }
+                    mmaCommit(&S.slotFull[k]);
+                }
+                if (!ok) break;
+                mmaCommit(&S.aEmpty[s]); // the tile's stage is free once its MMAs are done
+                if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[slot]);
+            }
+            mmaCommit(&S.mmaDone);
+            mbarWait(&S.mmaDone, 0, abortFlag, p.err, 44);
+        }
+        __syncwarp();
+    } else if (nT > 0 && warp >= 2 && warp < 2 + 2 * kTeamWarps) {
+        // ------------------------------------------------------------ epilogue teams
+        const uint32_t team = (warp - 2u) / kTeamWarps;
+        const uint32_t q = warp & 3u;
+        const uint32_t row = q * 32u + lane;
+        const uint32_t tRow = tmem + ((q * 32u) << 16);
+        const bool gather = p.perm != nullptr;
+        uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, uses0 = 0, uses1 = 0;
+        for (uint32_t t = 0; t < nT; t++) {
+            const TileInfo ti = tileAtSmem(S, p, t0, t);
+            if (ti.group != prevGroup) {
+                // every team waits for every group's block (see lookupPassTc)
+                slot ^= 1u;
+                const uint32_t u = slot ? uses1++ : uses0++;
+                if (!mbarWait(&S.bFull[slot], u & 1u, abortFlag, p.err, 50)) break;
+                prevGroup = ti.group;
+            }
+            if ((t & 1u) == team) {
+                const uint32_t orig = row < ti.count ? (gather ? __ldg(p.perm + ti.start + row) : ti.start + row) : 0u;
+                const uint32_t e = t % kNodeEntries;
+                if (!mbarWait(&S.nodeAcc[e], (t / kNodeEntries) & 1u, abortFlag, p.err, 51)) break;
+                tcFenceAfter();
+                uint32_t b;
+                {
+                    uint32_t r[16];
+                    tmemLoad16(tRow + kNodeCol0 + 16u * e, r);
+                    tmemWaitTie(r);
+                    b = argminScores(r, &S.cn[slot][0][0]);
+                }
+                tcFenceBefore();
+                __syncwarp();
+                if (lane == 0) mbarArrive(&S.nodeFree[e]);
+                if (!two) {
+                    if (row < ti.count) emitRow(S, p, smemHist, orig, ti.group * p.B + b);
+                } else {
+                    uint32_t sel[16];
+#pragma unroll
+                    for (int i = 0; i < 16; i++) sel[i] = 0;
+                    bool ok = true;
+                    for (uint32_t h = 0; h < nh; h++) {
+                        const uint32_t n = t * nh + h;
+                        const uint32_t k = n % kRingSlots;
+                        if (!mbarWait(&S.slotFull[k], (n / kRingSlots) & 1u, abortFlag, p.err, 52)) {
+                            ok = false;
+                            break;
+                        }
+                        tcFenceAfter();
+                        const uint32_t cb = h ? c0 : 0u;
+                        const uint32_t cnt = h ? p.B - c0 : c0;
+                        // child b's position in this half (0xFF: another half)
+                        const uint32_t rel = b - cb < cnt ? b - cb : 0xFFu;
+                        for (uint32_t c = 0; c < (16u * cnt + 63u) / 64u; c++) {
+                            uint32_t r[64];
+                            tmemLoad64(tRow + kSlotCols * k + 64u * c, r);
+                            tmemWaitTie64(r);
+#pragma unroll
+                            for (uint32_t kk = 0; kk < 4; kk++)
+#pragma unroll
+                                for (int i = 0; i < 16; i++) sel[i] = rel == 4u * c + kk ? r[16 * kk + i] : sel[i];
+                        }
+                        tcFenceBefore();
+                        __syncwarp();
+                        if (lane == 0) mbarArrive(&S.slotFree[k]);
+                    }
+                    if (!ok) break;
+                    if (row < ti.count) {
+                        const uint64_t child = uint64_t(ti.group) * p.B + b; // in-level index at level 2p+1
+                        const uint32_t b2 = argminScores(sel, &S.cn[slot][1 + b][0]);
+                        emitRow(S, p, smemHist, orig, static_cast<uint32_t>(child * p.B + b2));
+                    }
+                }
+            }
+            if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) {
+                __syncwarp();
+                if (lane == 0) mbarArrive(&S.bEmpty[slot]);
+            }
+        }
+    }
+
+    tcFenceBefore();
+    __syncthreads();
+    if (smemHist) {
+        for (uint32_t i = threadIdx.x; i < p.nbBins; i += blockDim.x) {
+            const uint32_t v = S.hist[i];
+            if (v) atomicAdd(&p.binCount[i], v);
+        }
+    }
+    if (warp == 0) {
+        tcFenceAfter();
+        tmemDealloc(tmem, kTmemCols);
+    }
+}
+
 // ------------------------------------------------------------------ regroup kernels
 // Exclusive scans of the bin histogram: rowOff = scan(count), tileOff = scan(ceil(count/128));
 // totals[0] = number of tiles, totals[1] = number of rows.
@@ -775,6 +1011,160 @@ __global__ void __launch_bounds__(kScatterThreads) scatterRows(const uint32_t* n
     }
 }
 
+// Regroup of at most kSmemHistMax bins in three kernels, without global atomics: regroupHist
+// counts each CTA's contiguous row range per bin (ctaHist[c][b]); regroupScan turns the counts
+// into the bins' totals, row and tile offsets and, in place, each (CTA, bin)'s first position;
+// regroupScatter hands out those positions again with shared-memory atomics.  Order inside a
+// bin is unspecified.
+constexpr uint32_t kRegroupThreads = 512;
+
+__device__ __forceinline__ void regroupRange(uint64_t n, uint64_t per, uint64_t& beg, uint64_t& end)
+{
+    beg = uint64_t(blockIdx.x) * per;
+    end = beg + per < n ? beg + per : n;
+    if (beg > end) beg = end;
+}
+
+// f(node, row) for every row of this CTA's range; four rows per 16-byte load, four loads in flight.
+template <typename F>
+__device__ __forceinline__ void forEachRow(const uint32_t* nodeNext, uint64_t beg, uint64_t end, F f)
+{
+    // per is a multiple of 16 rows, so beg is 64-byte aligned
+    const uint64_t nVec = (end - beg) / 4;
+    const uint4* v4 = reinterpret_cast<const uint4*>(nodeNext + beg);
+    uint64_t j = threadIdx.x;
+    for (; j + 3 * kRegroupThreads < nVec; j += 4 * kRegroupThreads) {
+        uint4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) v[u] = __ldg(v4 + j + u * kRegroupThreads);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint64_t r = beg + 4 * (j + u * kRegroupThreads);
+            f(v[u].x, r);
+            f(v[u].y, r + 1);
+            f(v[u].z, r + 2);
+            f(v[u].w, r + 3);
+        }
+    }
+    for (; j < nVec; j += kRegroupThreads) {
+        const uint4 v = __ldg(v4 + j);
+        const uint64_t r = beg + 4 * j;
+        f(v.x, r);
+        f(v.y, r + 1);
+        f(v.z, r + 2);
+        f(v.w, r + 3);
+    }
+    for (uint64_t r = beg + 4 * nVec + threadIdx.x; r < end; r += kRegroupThreads) f(__ldg(nodeNext + r), r);
+}
+
+__global__ void __launch_bounds__(kRegroupThreads) regroupHist(const uint32_t* nodeNext, uint64_t n, uint64_t per,
+                                                               uint32_t nb, uint32_t* ctaHist)
+{
+    __shared__ uint32_t hist[kSmemHistMax];
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    uint64_t beg, end;
+    regroupRange(n, per, beg, end);
+    forEachRow(nodeNext, beg, end, [&](uint32_t node, uint64_t) { atomicAdd(&hist[node], 1u); });
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) ctaHist[uint64_t(blockIdx.x) * nb + i] = hist[i];
+}
+
+// One CTA of 1024 threads: thread (k, b) owns bin b's CTAs [k * len, (k + 1) * len).
+__global__ void __launch_bounds__(1024) regroupScan(uint32_t* ctaHist, uint32_t nCta, uint32_t nb, uint32_t* count,
+                                                    uint32_t* rowOff, uint32_t* tileOff, uint32_t* totals)
+{
+    __shared__ uint32_t part[1024];
+    __shared__ uint32_t wa[32], wb[32];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, w = tid >> 5;
+    const uint32_t chunks = 1024 / nb;                    // >= 1 (nb <= 1024)
+    const uint32_t len = (nCta + chunks - 1) / chunks;
+    const uint32_t b = tid % nb, k = tid / nb;
+    const bool active = k < chunks;
+    const uint32_t c0 = active ? k * len : nCta;
+    const uint32_t c1 = active ? min(nCta, c0 + len) : nCta;
+    uint32_t sum = 0;
+    for (uint32_t c = c0; c < c1; c++) sum += ctaHist[uint64_t(c) * nb + b];
+    part[tid] = sum;
+    __syncthreads();
+    // bin totals and the chunk's prefix inside its bin
+    uint32_t before = 0, total = 0;
+    if (active) {
+        for (uint32_t kk = 0; kk < chunks; kk++) {
+            const uint32_t v = part[kk * nb + b];
+            if (kk < k) before += v;
+            total += v;
+        }
+    }
+    // exclusive scans over bins of total and ceil(total / 128) (threads k == 0 hold the bins)
+    const bool owner = active && k == 0;
+    const uint32_t ca = owner ? total : 0u, cb = owner ? (total + kTileRows - 1) / kTileRows : 0u;
+    uint32_t a = ca, t = cb;
+#pragma unroll
+    for (uint32_t off = 1; off < 32; off <<= 1) {
+        const uint32_t xa = __shfl_up_sync(0xFFFFFFFFu, a, off);
+        const uint32_t xb = __shfl_up_sync(0xFFFFFFFFu, t, off);
+        if (lane >= off) {
+            a += xa;
+            t += xb;
+        }
+    }
+    if (lane == 31) {
+        wa[w] = a;
+        wb[w] = t;
+    }
+    __syncthreads();
+    if (w == 0) {
+        uint32_t va = wa[lane], vb = wb[lane];
+#pragma unroll
+        for (uint32_t off = 1; off < 32; off <<= 1) {
+            const uint32_t xa = __shfl_up_sync(0xFFFFFFFFu, va, off);
+            const uint32_t xb = __shfl_up_sync(0xFFFFFFFFu, vb, off);
+            if (lane >= off) {
+                va += xa;
+                vb += xb;
+            }
+        }
+        wa[lane] = va;
+        wb[lane] = vb;
+    }
+    __syncthreads();
+    const uint32_t exA = (w ? wa[w - 1] : 0u) + a - ca;
+    const uint32_t exB = (w ? wb[w - 1] : 0u) + t - cb;
+    if (owner) {
+        count[b] = total;
+        rowOff[b] = exA;
+        tileOff[b] = exB;
+        part[b] = exA; // the bin's first row, for the other chunks (read after the barrier)
+    }
+    if (tid == 1023) {
+        totals[0] = wb[31];
+        totals[1] = wa[31];
+    }
+    __syncthreads();
+    if (active) {
+        uint32_t run = part[b] + before;
+        for (uint32_t c = c0; c < c1; c++) {
+            const uint64_t i = uint64_t(c) * nb + b;
+            const uint32_t v = ctaHist[i];
+            ctaHist[i] = run;
+            run += v;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kRegroupThreads) regroupScatter(const uint32_t* nodeNext, uint64_t n, uint64_t per,
+                                                                  uint32_t nb, const uint32_t* ctaOff, uint32_t* perm)
+{
+    __shared__ uint32_t next[kSmemHistMax];
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) next[i] = ctaOff[uint64_t(blockIdx.x) * nb + i];
+    __syncthreads();
+    uint64_t beg, end;
+    regroupRange(n, per, beg, end);
+    forEachRow(nodeNext, beg, end,
+               [&](uint32_t node, uint64_t r) { perm[atomicAdd(&next[node], 1u)] = static_cast<uint32_t>(r); });
+}
+
 // ------------------------------------------------------------------ plain FP32 SIMT kernel
 // One thread per descriptor.  The block's 128 descriptor rows are staged once in shared memory
 // (coalesced 16-byte loads; rows padded to 144 bytes so that the eight 16-byte reads of a
@@ -899,6 +1289,18 @@ uint32_t maxBinsFor(uint32_t B, uint32_t L)
     return static_cast<uint32_t>(m);
 }
 
+// Words of the per-CTA histograms: regroups of at most kSmemHistMax bins use them.
+uint64_t ctaHistWords(uint32_t B, uint32_t L)
+{
+    uint64_t m = 0;
+    const uint32_t passes = (L + 1) / 2;
+    for (uint32_t p = 0; p + 1 < passes; p++) {
+        const uint64_t nb = ipow(B, 2 * p + 2);
+        if (nb <= kSmemHistMax) m = std::max<uint64_t>(m, nb);
+    }
+    return m * kRegroupCtas;
+}
+
 } // namespace
 
 size_t lookupScratchBytes(uint32_t B, uint32_t L, uint64_t n)
@@ -907,7 +1309,8 @@ size_t lookupScratchBytes(uint32_t B, uint32_t L, uint64_t n)
     const uint64_t bins = maxBinsFor(B, L);
     const uint64_t tiles = n / kTileRows + bins + 1;
     auto a = [](uint64_t b) { return (b + 255) / 256 * 256; };
-    return a(sizeof(DeviceErrors)) + 2 * a(n * 4) + a((4 * bins + 4) * 4) + a(tiles * sizeof(TileInfo));
+    return a(sizeof(DeviceErrors)) + 2 * a(n * 4) + a((4 * bins + 4) * 4) + a(tiles * sizeof(TileInfo)) +
+           a(ctaHistWords(B, L) * 4);
 }
 
 LookupScratch carveLookupScratch(void* base, uint32_t B, uint32_t L, uint64_t n)
@@ -926,6 +1329,8 @@ LookupScratch carveLookupScratch(void* base, uint32_t B, uint32_t L, uint64_t n)
     s.bins = reinterpret_cast<uint32_t*>(p);
     p += a((4 * bins + 4) * 4);
     s.tiles = p;
+    p += a((n / kTileRows + bins + 1) * sizeof(TileInfo));
+    s.ctaHist = reinterpret_cast<uint32_t*>(p);
     return s;
 }
 
@@ -942,8 +1347,12 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
         return 1;
     }
     const bool warpNode = algo == kLookupTensorU8WarpNode;
-    static std::atomic<uint64_t> attrSet{0}, attrSetW{0};
-    if (warpNode) {
+    const bool ring = algo == kLookupTensorU8Ring;
+    static std::atomic<uint64_t> attrSet{0}, attrSetW{0}, attrSetR{0};
+    if (ring) {
+        setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(lookupPassRing),
+                                       static_cast<int>(kTcSmemBytes), attrSetR);
+    } else if (warpNode) {
         setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(lookupPassTc<true>),
                                        static_cast<int>(kTcSmemBytes), attrSetW);
     } else {
@@ -981,18 +1390,23 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
             p.nTilesDev = totals;
         }
         uint32_t nbBins = 0;
+        // regroups of at most kSmemHistMax bins count per CTA in regroupHist; larger ones in the pass
+        bool ctaRegroup = false;
         if (p.isFinal) {
             p.out = leaf;
         } else {
             nbBins = static_cast<uint32_t>(ipow(B, 2 * pass + 2));
+            ctaRegroup = nbBins <= kSmemHistMax && scratch.ctaHist != nullptr;
             p.nodeNext = scratch.nodeNext;
-            p.binCount = count;
+            p.binCount = ctaRegroup ? nullptr : count;
             p.nbBins = nbBins;
-            RBW_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t) * nbBins, stream));
+            if (!ctaRegroup) RBW_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t) * nbBins, stream));
         }
         {
             ScopedKernelTimer timer(kTimedLookupPass, stream);
-            if (warpNode) {
+            if (ring) {
+                lookupPassRing<<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
+            } else if (warpNode) {
                 lookupPassTc<true><<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
             } else {
                 lookupPassTc<false><<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
@@ -1002,9 +1416,22 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
         kernels++;
         if (!p.isFinal) {
             ScopedKernelTimer timer(kTimedRegroup, stream);
+            const uint32_t tileBlocks = std::min<uint32_t>((maxTiles + 255) / 256, 4096);
+            if (ctaRegroup) {
+                const uint64_t per = ((n + kRegroupCtas - 1) / kRegroupCtas + 15) / 16 * 16;
+                regroupHist<<<kRegroupCtas, kRegroupThreads, 0, stream>>>(scratch.nodeNext, n, per, nbBins,
+                                                                         scratch.ctaHist);
+                regroupScan<<<1, 1024, 0, stream>>>(scratch.ctaHist, kRegroupCtas, nbBins, count, rowOff, tileOff,
+                                                    totals);
+                buildTiles<<<tileBlocks, 256, 0, stream>>>(count, rowOff, tileOff, nbBins, totals, maxTiles, tiles);
+                regroupScatter<<<kRegroupCtas, kRegroupThreads, 0, stream>>>(scratch.nodeNext, n, per, nbBins,
+                                                                            scratch.ctaHist, scratch.perm);
+                RBW_CUDA(cudaGetLastError());
+                kernels += 4;
+                continue;
+            }
             scanBins<<<1, 1024, 0, stream>>>(count, nbBins, rowOff, tileOff, totals);
             RBW_CUDA(cudaGetLastError());
-            const uint32_t tileBlocks = std::min<uint32_t>((maxTiles + 255) / 256, 4096);
             buildTiles<<<tileBlocks, 256, 0, stream>>>(count, rowOff, tileOff, nbBins, totals, maxTiles, tiles);
             RBW_CUDA(cudaGetLastError());
             RBW_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nbBins, stream));

@@ -20,6 +20,8 @@ enum LookupAlgo : int {
     kLookupTensorU8 = 1, // tcgen05 kind::i8, level pairs + counting-sort regroup
     kLookupSimtF32 = 2,  // plain FP32 SIMT kernel (the comparison baseline)
     kLookupTensorU8WarpNode = 3, // as kLookupTensorU8, the node level of each pair by warp-level MMAs
+    kLookupTensorU8Ring = 4,     // as kLookupTensorU8, one MMA issuer with a three-slot accumulator ring
+    kLookupAlgoLast = kLookupTensorU8Ring,
 };
 
 struct LookupStats {
@@ -33,6 +35,7 @@ struct LookupScratch {
     uint32_t* perm = nullptr;     // [n]
     uint32_t* bins = nullptr;     // [4 * maxBins + 4] : count | rowOff | tileOff | cursor | total
     void* tiles = nullptr;        // [maxTiles] TileInfo
+    uint32_t* ctaHist = nullptr;  // [regroup CTAs][bins] per-CTA bin counts, then their offsets
     DeviceErrors* err = nullptr;
 };
 

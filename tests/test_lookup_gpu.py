@@ -9,7 +9,7 @@ from tests.helpers import edge_descriptors, random_tree
 
 pytestmark = pytest.mark.gpu
 
-ALGOS = ["tensor_u8", "simt_f32", "tensor_u8_warpnode"]
+ALGOS = ["tensor_u8", "simt_f32", "tensor_u8_warpnode", "tensor_u8_ring"]
 
 
 def _lookup(voc, desc_np, algo):
@@ -42,6 +42,7 @@ def test_lookup_sizes_tensor_vs_simt_vs_oracle(oracle, n):
     b = _lookup(voc, desc, "simt_f32")
     assert np.array_equal(a, b)
     assert np.array_equal(_lookup(voc, desc, "tensor_u8_warpnode"), b)
+    assert np.array_equal(_lookup(voc, desc, "tensor_u8_ring"), b)
     assert np.array_equal(a, oracle.lookup(centers, B, L, desc, threads=8))
 
 
@@ -133,7 +134,7 @@ def test_lookup_repeated_large_batches_are_exact():
     voc = rbw.build_vocabulary(train, 16, nb_doc=1000, nb_levels=4, init="kmeans++", seed=5, max_iterations=5)
     desc = sift_like(8_000_000, seed=22, device="cuda")
     want = voc.lookup(desc, algo="simt_f32")
-    for algo in ("tensor_u8", "tensor_u8_warpnode"):
+    for algo in ("tensor_u8", "tensor_u8_warpnode", "tensor_u8_ring"):
         for _ in range(4):
             got = voc.lookup(desc, algo=algo)
             torch.cuda.synchronize()
