@@ -49,6 +49,8 @@ namespace {
 constexpr uint32_t kMaxDocDesc = 32768;   // descriptors sorted in shared memory; larger ones in global memory
 constexpr uint32_t kPrepThreads = 512;
 constexpr uint32_t kScoreThreads = 1024;
+constexpr uint32_t kFlatList = 256;        // leaf lists shorter than this are walked flattened per warp batch
+constexpr uint32_t kFlatDepth = 8;         // pairs per lane in flight in the flattened walk
 constexpr uint32_t kSegThreads = 256;
 constexpr uint32_t kSmemDocs = 20480;     // per-document accumulators kept in shared memory
 constexpr uint64_t kShardTableMinBytes = 64ull << 20; // per-shard CSR tables always allowed up to this size
@@ -494,84 +496,125 @@ __global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
     const Entry* ent = P.entries + (P.qOff[q] - P.qOff[0]) * P.L;
     const uint32_t ne = P.entryCount[q];
     const float qRcp = P.qRcpF[q];
-    for (uint32_t e = warp; e < ne; e += nWarpsCta) {
-        const Entry en = ent[e];
-        const float w = P.weights[en.widx];
-        const float qv = float(en.run) * w * qRcp;
-        const bool leafLevel = en.level == P.L - 1;
-        const uint64_t span = ipowDev(P.B, P.L - 1 - en.level);
+    // this shard's offset tables in the two segments (nullptr: the segment holds none of its documents)
+    const uint32_t* segOff[2];
 #pragma unroll
-        for (int s = 0; s < 2; s++) {
-            const uint64_t* pairs = P.seg[s].pairs;
-            const uint32_t* leafOff = P.seg[s].leafOff;
-            if (P.seg[s].stride) {
-                // this shard's own inverted file (none: the segment holds no document of it)
-                const uint32_t rel = shard - P.seg[s].shardBeg;
-                if (rel >= P.seg[s].nShards) continue;
-                leafOff += uint64_t(rel) * P.seg[s].stride;
+    for (int s = 0; s < 2; s++) {
+        segOff[s] = P.seg[s].leafOff;
+        if (P.seg[s].stride) {
+            const uint32_t rel = shard - P.seg[s].shardBeg;
+            segOff[s] = rel < P.seg[s].nShards ? segOff[s] + uint64_t(rel) * P.seg[s].stride : nullptr;
+        }
+    }
+    auto addPair = [&](uint64_t pr, float qv) {
+        const uint32_t i = static_cast<uint32_t>(pr >> 32) - docBeg;
+        if (!kSharded || i < nLocal) addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
+    };
+    // A leaf word's list [a, b) by the whole warp, eight pairs per lane in flight.
+    auto leafList = [&](const uint64_t* pairs, uint32_t a, uint32_t b, float qv) {
+        uint32_t p = a + lane;
+        for (; p + 224 < b; p += 256) {
+            uint64_t pr[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) pr[u] = pairs[p + 32 * u];
+#pragma unroll
+            for (int u = 0; u < 8; u++) addPair(pr[u], qv);
+        }
+        for (; p < b; p += 32) addPair(pairs[p], qv);
+    };
+    // Virtual inverted file of a non-leaf word: the union of the leaf lists below it, counted
+    // per document (DataBase.cpp:150-164).  A document lives in one segment only, and the skip
+    // rule keeps the union short, so each lane scans the range for the documents of this shard
+    // whose first pair it holds.
+    auto virtualList = [&](int s, uint32_t a, uint32_t b, float w, float qv) {
+        const uint64_t* pairs = P.seg[s].pairs;
+        for (uint32_t p = a + lane; p < b; p += 32) {
+            const uint32_t slot = static_cast<uint32_t>(pairs[p] >> 32);
+            if (kSharded && slot - docBeg >= nLocal) continue;
+            bool first = true;
+            for (uint32_t r = a; r < p && first; r++) first = static_cast<uint32_t>(pairs[r] >> 32) != slot;
+            if (!first) continue;
+            uint32_t tf = 0;
+            for (uint32_t r = p; r < b; r++)
+                if (static_cast<uint32_t>(pairs[r] >> 32) == slot) tf += P.seg[s].tf[r];
+            const float d = float(tf) * w * P.rcpF[slot];
+            addTerm(acc, touched, slot - docBeg, termOf(qv, d));
+        }
+    };
+    // Entries in batches of 32 per warp: lane j fetches entry base + j, its weight and its
+    // offsets in both segments, so these loads overlap instead of chaining entry after entry.
+    // Leaf lists shorter than kFlatList are then walked as one range over the batch (lane t of
+    // a round takes pair t of the concatenated lists, kFlatDepth pairs per lane in flight);
+    // longer lists and non-leaf words go one at a time with the whole warp.
+    for (uint32_t base = warp * 32u; base < ne; base += nWarpsCta * 32u) {
+        const uint32_t e = base + lane;
+        const bool valid = e < ne;
+        uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+        float qv = 0.f, w = 0.f;
+        bool leaf = false;
+        if (valid) {
+            const Entry en = ent[e];
+            w = P.weights[en.widx];
+            qv = float(en.run) * w * qRcp;
+            leaf = en.level == P.L - 1;
+            const uint64_t span = ipowDev(P.B, P.L - 1 - en.level);
+            if (segOff[0] != nullptr) {
+                a0 = segOff[0][uint64_t(en.word) * span];
+                b0 = segOff[0][(uint64_t(en.word) + 1) * span];
             }
-            const uint32_t a = leafOff[uint64_t(en.word) * span];
-            const uint32_t b = leafOff[(uint64_t(en.word) + 1) * span];
-            if (leafLevel) {
-                // sixteen pairs per lane in flight
-                uint32_t p = a + lane;
-                for (; p + 480 < b; p += 512) {
-                    uint64_t pr[16];
-#pragma unroll
-                    for (int u = 0; u < 16; u++) pr[u] = pairs[p + 32 * u];
-#pragma unroll
-                    for (int u = 0; u < 16; u++) {
-                        const uint32_t i = static_cast<uint32_t>(pr[u] >> 32) - docBeg;
-                        if (!kSharded || i < nLocal)
-                            addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
-                    }
-                }
-                for (; p + 224 < b; p += 256) {
-                    uint64_t pr[8];
-#pragma unroll
-                    for (int u = 0; u < 8; u++) pr[u] = pairs[p + 32 * u];
-#pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        const uint32_t i = static_cast<uint32_t>(pr[u] >> 32) - docBeg;
-                        if (!kSharded || i < nLocal)
-                            addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
-                    }
-                }
-                for (; p + 96 < b; p += 128) {
-                    uint64_t pr[4];
-#pragma unroll
-                    for (int u = 0; u < 4; u++) pr[u] = pairs[p + 32 * u];
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const uint32_t i = static_cast<uint32_t>(pr[u] >> 32) - docBeg;
-                        if (!kSharded || i < nLocal)
-                            addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr[u]))));
-                    }
-                }
-                for (; p < b; p += 32) {
-                    const uint64_t pr = pairs[p];
-                    const uint32_t i = static_cast<uint32_t>(pr >> 32) - docBeg;
-                    if (!kSharded || i < nLocal)
-                        addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
-                }
+            if (segOff[1] != nullptr) {
+                a1 = segOff[1][uint64_t(en.word) * span];
+                b1 = segOff[1][(uint64_t(en.word) + 1) * span];
+            }
+        }
+        const uint32_t len = (b0 - a0) + (b1 - a1);
+        const bool flat = valid && leaf && len < kFlatList;
+        for (uint32_t one = __ballot_sync(0xFFFFFFFFu, valid && !flat); one != 0; one &= one - 1) {
+            const uint32_t j = __ffs(one) - 1;
+            const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), jb0 = __shfl_sync(0xFFFFFFFFu, b0, j);
+            const uint32_t ja1 = __shfl_sync(0xFFFFFFFFu, a1, j), jb1 = __shfl_sync(0xFFFFFFFFu, b1, j);
+            const float jq = __shfl_sync(0xFFFFFFFFu, qv, j), jw = __shfl_sync(0xFFFFFFFFu, w, j);
+            if (__shfl_sync(0xFFFFFFFFu, leaf, j)) {
+                leafList(P.seg[0].pairs, ja0, jb0, jq);
+                leafList(P.seg[1].pairs, ja1, jb1, jq);
             } else {
-                // Virtual inverted file of a non-leaf word: the union of the leaf lists below
-                // it, counted per document (DataBase.cpp:150-164).  A document lives in one
-                // segment only, and the skip rule keeps the union short, so each lane scans the
-                // segment's range for the documents of this shard whose first pair it holds.
-                for (uint32_t p = a + lane; p < b; p += 32) {
-                    const uint32_t slot = static_cast<uint32_t>(pairs[p] >> 32);
-                    if (kSharded && slot - docBeg >= nLocal) continue;
-                    bool first = true;
-                    for (uint32_t r = a; r < p && first; r++) first = static_cast<uint32_t>(pairs[r] >> 32) != slot;
-                    if (!first) continue;
-                    uint32_t tf = 0;
-                    for (uint32_t r = p; r < b; r++)
-                        if (static_cast<uint32_t>(pairs[r] >> 32) == slot) tf += P.seg[s].tf[r];
-                    const float d = float(tf) * w * P.rcpF[slot];
-                    addTerm(acc, touched, slot - docBeg, termOf(qv, d));
-                }
+                virtualList(0, ja0, jb0, jw, jq);
+                virtualList(1, ja1, jb1, jw, jq);
             }
+        }
+        const uint32_t c0 = flat ? b0 - a0 : 0u;
+        const uint32_t cnt = flat ? len : 0u;
+        uint32_t incl = cnt;
+#pragma unroll
+        for (uint32_t off = 1; off < 32; off <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+            if (lane >= off) incl += v;
+        }
+        const uint32_t excl = incl - cnt;
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        for (uint32_t t0 = 0; t0 < total; t0 += 32u * kFlatDepth) {
+            uint64_t pr[kFlatDepth];
+            float pq[kFlatDepth];
+#pragma unroll
+            for (uint32_t u = 0; u < kFlatDepth; u++) {
+                const uint32_t t = t0 + 32u * u + lane;
+                // owner lane: the last j with excl_j <= t (excl is non-decreasing; it holds pairs)
+                uint32_t j = 0;
+#pragma unroll
+                for (uint32_t step = 16; step > 0; step >>= 1) {
+                    const uint32_t v = __shfl_sync(0xFFFFFFFFu, excl, j + step);
+                    if (v <= t) j += step;
+                }
+                const uint32_t off = t - __shfl_sync(0xFFFFFFFFu, excl, j);
+                const uint32_t jc0 = __shfl_sync(0xFFFFFFFFu, c0, j);
+                const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), ja1 = __shfl_sync(0xFFFFFFFFu, a1, j);
+                pq[u] = __shfl_sync(0xFFFFFFFFu, qv, j);
+                pr[u] = 0;
+                if (t < total) pr[u] = off < jc0 ? P.seg[0].pairs[ja0 + off] : P.seg[1].pairs[ja1 + off - jc0];
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < kFlatDepth; u++)
+                if (t0 + 32u * u + lane < total) addPair(pr[u], pq[u]);
         }
     }
     __syncthreads();

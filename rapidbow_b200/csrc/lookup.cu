@@ -39,7 +39,7 @@ constexpr uint32_t kTeamWarps = 4;                    // epilogue team: one warp
 constexpr uint32_t kIssuer1Warp = 2 + 2 * kTeamWarps;        // second MMA issuer, after the teams
 constexpr uint32_t kTcThreads = 32 * (3 + 2 * kTeamWarps); // TMA, two MMA issuers, two epilogue teams
 constexpr uint32_t kSmemHistMax = 1024;
-constexpr uint32_t kRegroupCtas = 296;                // regroup kernels' CTAs (2 per SM on 148 SMs)
+constexpr uint32_t kRegroupCtas = 148;                // regroup kernels' CTAs (one per SM on 148 SMs)
 // Two accumulator buffers of 256 columns; tile t uses buffer t & 1.  Its level-2p MMA (16
 // columns) lands in the first columns of the buffer and is read by the buffer's epilogue team
 // before the children MMA of the same tile overwrites the buffer.
@@ -1016,7 +1016,7 @@ __global__ void __launch_bounds__(kScatterThreads) scatterRows(const uint32_t* n
 // into the bins' totals, row and tile offsets and, in place, each (CTA, bin)'s first position;
 // regroupScatter hands out those positions again with shared-memory atomics.  Order inside a
 // bin is unspecified.
-constexpr uint32_t kRegroupThreads = 512;
+constexpr uint32_t kRegroupThreads = 1024;
 
 __device__ __forceinline__ void regroupRange(uint64_t n, uint64_t per, uint64_t& beg, uint64_t& end)
 {
