@@ -372,7 +372,7 @@ enum {
     RBW_TUNE_ASSIGN_F32_CTAS_PER_SM = 1, /* float-center assign: CTAs per SM, 1..3 (default 3) */
     RBW_TUNE_SCATTER_ROWS = 2,           /* lookup regroup: rows per thread, 8, 16 or 32 (default 16) */
     RBW_TUNE_DB_SHARD_TABLES = 3         /* DataBase inverted file, keyed by documents instead of
-                                            descriptors: 1 one CSR per 20,480-document shard while
+                                            descriptors: 1 one CSR per 2,560-document shard while
                                             those tables stay small (default), 2 one CSR */
 };
 /* value 0 removes the entry; RBW_ERR_INVALID_ARG for a value the parameter cannot take. */

@@ -8,7 +8,7 @@ tree levels, descriptor-count bucket = floor(log2(n))):
     assign_ctas_per_sm      uint8 k-means assign, CTAs per SM: 2..6         (default 6)
     assign_f32_ctas_per_sm  float-center assign, CTAs per SM: 1..3          (default 3)
     scatter_rows            lookup regroup scatter, rows per thread: 8|16|32 (default 16)
-    db_shard_tables         DataBase inverted file: 1 one CSR per 20,480-document shard while
+    db_shard_tables         DataBase inverted file: 1 one CSR per 2,560-document shard while
                             small, 2 one CSR (default 1; its bucket counts documents)
 
 Cache file (JSON): {"format": "rapidbow_b200 tuning cache", "version": 1,

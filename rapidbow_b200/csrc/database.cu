@@ -53,6 +53,7 @@ constexpr uint32_t kFlatList = 256;        // leaf lists shorter than this are w
 constexpr uint32_t kFlatDepth = 8;         // pairs per lane in flight in the flattened walk
 constexpr uint32_t kSegThreads = 256;
 constexpr uint32_t kSmemDocs = 20480;     // per-document accumulators kept in shared memory
+constexpr uint32_t kShardDocs = 2560;     // documents per inverted-file shard (kSmemDocs / 8)
 constexpr uint64_t kShardTableMinBytes = 64ull << 20; // per-shard CSR tables always allowed up to this size
 constexpr uint32_t kMaxK = 1024;          // results selected in shared memory; more in global memory
 constexpr double kFixScale = 72057594037927936.0; // 2^56
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(kPrepThreads) docPrepKernel(const uint32_t* ne
 // (stride = leaves per shard table), or the single table (stride 0).
 __device__ __forceinline__ uint64_t segRow(uint32_t slot, uint32_t shardBeg, uint64_t stride)
 {
-    return stride ? uint64_t(slot / kSmemDocs - shardBeg) * stride : 0ull;
+    return stride ? uint64_t(slot / kShardDocs - shardBeg) * stride : 0ull;
 }
 
 // Per-(shard, leaf) pair counts and per-leaf posting counts of the documents [s0, s0 + gridDim.x).
@@ -353,7 +354,7 @@ struct SegmentView {
     const uint32_t* leafOff;   // [nShards * stride + 1], or [nbLeaves + 1] when stride = 0
     const uint64_t* pairs;     // slot << 32 | float bits of the leaf-level document entry
     const uint32_t* tf;        // descriptors of the document under the leaf
-    uint64_t stride;           // nbLeaves: one CSR per shard of kSmemDocs slots; 0: one CSR
+    uint64_t stride;           // nbLeaves: one CSR per shard of kShardDocs slots; 0: one CSR
     uint32_t shardBeg, nShards;
 };
 
@@ -364,6 +365,7 @@ struct ScoreParams {
     const float* qRcpF;
     const float* weights;
     SegmentView seg[2];        // main, delta
+    uint32_t csrPerCta;        // inverted-file shards per CTA (segments with per-shard CSRs), else 1
     const float* rcpF;
     const uint32_t* slotDoc;
     uint32_t nDocs;
@@ -465,13 +467,13 @@ __device__ __forceinline__ void writeResults(const ScoreParams& P, uint32_t q, c
     if (threadIdx.x == 0) P.outCount[q] = want;
 }
 
-// One CTA per (query, shard of shardDocs documents).  The accumulators of the shard live in
-// shared memory (9 B per document).  A segment indexed per shard hands each CTA the postings
-// of its own shard; a segment with one inverted file (stride 0) is walked by every CTA of the
-// query, each keeping the postings of its shard.  kSharded = false: one shard holds every
-// document and no posting needs the shard test.
-template <bool kSharded>
-__global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
+// One CTA per (query, range of shardDocs documents).  The accumulators of the range live in
+// shared memory (9 B per document).  Segments indexed per shard of kShardDocs documents hand
+// the CTA the postings of its csrPerCta shards only; a segment with one inverted file (stride 0)
+// is walked by every CTA of the query, each keeping the postings of its range.  kSharded =
+// false: one range holds every document and no posting needs the range test.
+template <bool kSharded, uint32_t kThreads>
+__global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThreads) scoreKernel(ScoreParams P)
 {
     extern __shared__ unsigned long long dyn[];
     __shared__ uint32_t nTouched;
@@ -496,16 +498,13 @@ __global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
     const Entry* ent = P.entries + (P.qOff[q] - P.qOff[0]) * P.L;
     const uint32_t ne = P.entryCount[q];
     const float qRcp = P.qRcpF[q];
-    // this shard's offset tables in the two segments (nullptr: the segment holds none of its documents)
-    const uint32_t* segOff[2];
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-        segOff[s] = P.seg[s].leafOff;
-        if (P.seg[s].stride) {
-            const uint32_t rel = shard - P.seg[s].shardBeg;
-            segOff[s] = rel < P.seg[s].nShards ? segOff[s] + uint64_t(rel) * P.seg[s].stride : nullptr;
-        }
-    }
+    // Offset table of inverted-file shard `csr` in segment s (nullptr: the segment holds none of
+    // its documents); a one-table segment is walked once, as sub-table 0.
+    auto subTable = [&](int s, uint32_t sub) -> const uint32_t* {
+        if (P.seg[s].stride == 0) return sub == 0 ? P.seg[s].leafOff : nullptr;
+        const uint32_t rel = shard * P.csrPerCta + sub - P.seg[s].shardBeg;
+        return rel < P.seg[s].nShards ? P.seg[s].leafOff + uint64_t(rel) * P.seg[s].stride : nullptr;
+    };
     auto addPair = [&](uint64_t pr, float qv) {
         const uint32_t i = static_cast<uint32_t>(pr >> 32) - docBeg;
         if (!kSharded || i < nLocal) addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
@@ -549,72 +548,79 @@ __global__ void __launch_bounds__(kScoreThreads, 1) scoreKernel(ScoreParams P)
     for (uint32_t base = warp * 32u; base < ne; base += nWarpsCta * 32u) {
         const uint32_t e = base + lane;
         const bool valid = e < ne;
-        uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
         float qv = 0.f, w = 0.f;
         bool leaf = false;
+        uint64_t lo = 0, hi = 0; // the word's leaf range
         if (valid) {
             const Entry en = ent[e];
             w = P.weights[en.widx];
             qv = float(en.run) * w * qRcp;
             leaf = en.level == P.L - 1;
             const uint64_t span = ipowDev(P.B, P.L - 1 - en.level);
-            if (segOff[0] != nullptr) {
-                a0 = segOff[0][uint64_t(en.word) * span];
-                b0 = segOff[0][(uint64_t(en.word) + 1) * span];
-            }
-            if (segOff[1] != nullptr) {
-                a1 = segOff[1][uint64_t(en.word) * span];
-                b1 = segOff[1][(uint64_t(en.word) + 1) * span];
-            }
+            lo = uint64_t(en.word) * span;
+            hi = lo + span;
         }
-        const uint32_t len = (b0 - a0) + (b1 - a1);
-        const bool flat = valid && leaf && len < kFlatList;
-        for (uint32_t one = __ballot_sync(0xFFFFFFFFu, valid && !flat); one != 0; one &= one - 1) {
-            const uint32_t j = __ffs(one) - 1;
-            const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), jb0 = __shfl_sync(0xFFFFFFFFu, b0, j);
-            const uint32_t ja1 = __shfl_sync(0xFFFFFFFFu, a1, j), jb1 = __shfl_sync(0xFFFFFFFFu, b1, j);
-            const float jq = __shfl_sync(0xFFFFFFFFu, qv, j), jw = __shfl_sync(0xFFFFFFFFu, w, j);
-            if (__shfl_sync(0xFFFFFFFFu, leaf, j)) {
-                leafList(P.seg[0].pairs, ja0, jb0, jq);
-                leafList(P.seg[1].pairs, ja1, jb1, jq);
-            } else {
-                virtualList(0, ja0, jb0, jw, jq);
-                virtualList(1, ja1, jb1, jw, jq);
+        for (uint32_t sub = 0; sub < P.csrPerCta; sub++) {
+            uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+            const uint32_t* t0 = subTable(0, sub);
+            const uint32_t* t1 = subTable(1, sub);
+            if (valid && t0 != nullptr) {
+                a0 = t0[lo];
+                b0 = t0[hi];
             }
-        }
-        const uint32_t c0 = flat ? b0 - a0 : 0u;
-        const uint32_t cnt = flat ? len : 0u;
-        uint32_t incl = cnt;
-#pragma unroll
-        for (uint32_t off = 1; off < 32; off <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
-            if (lane >= off) incl += v;
-        }
-        const uint32_t excl = incl - cnt;
-        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        for (uint32_t t0 = 0; t0 < total; t0 += 32u * kFlatDepth) {
-            uint64_t pr[kFlatDepth];
-            float pq[kFlatDepth];
-#pragma unroll
-            for (uint32_t u = 0; u < kFlatDepth; u++) {
-                const uint32_t t = t0 + 32u * u + lane;
-                // owner lane: the last j with excl_j <= t (excl is non-decreasing; it holds pairs)
-                uint32_t j = 0;
-#pragma unroll
-                for (uint32_t step = 16; step > 0; step >>= 1) {
-                    const uint32_t v = __shfl_sync(0xFFFFFFFFu, excl, j + step);
-                    if (v <= t) j += step;
+            if (valid && t1 != nullptr) {
+                a1 = t1[lo];
+                b1 = t1[hi];
+            }
+            const uint32_t len = (b0 - a0) + (b1 - a1);
+            const bool flat = valid && leaf && len < kFlatList;
+            for (uint32_t one = __ballot_sync(0xFFFFFFFFu, valid && !flat); one != 0; one &= one - 1) {
+                const uint32_t j = __ffs(one) - 1;
+                const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), jb0 = __shfl_sync(0xFFFFFFFFu, b0, j);
+                const uint32_t ja1 = __shfl_sync(0xFFFFFFFFu, a1, j), jb1 = __shfl_sync(0xFFFFFFFFu, b1, j);
+                const float jq = __shfl_sync(0xFFFFFFFFu, qv, j), jw = __shfl_sync(0xFFFFFFFFu, w, j);
+                if (__shfl_sync(0xFFFFFFFFu, leaf, j)) {
+                    leafList(P.seg[0].pairs, ja0, jb0, jq);
+                    leafList(P.seg[1].pairs, ja1, jb1, jq);
+                } else {
+                    virtualList(0, ja0, jb0, jw, jq);
+                    virtualList(1, ja1, jb1, jw, jq);
                 }
-                const uint32_t off = t - __shfl_sync(0xFFFFFFFFu, excl, j);
-                const uint32_t jc0 = __shfl_sync(0xFFFFFFFFu, c0, j);
-                const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), ja1 = __shfl_sync(0xFFFFFFFFu, a1, j);
-                pq[u] = __shfl_sync(0xFFFFFFFFu, qv, j);
-                pr[u] = 0;
-                if (t < total) pr[u] = off < jc0 ? P.seg[0].pairs[ja0 + off] : P.seg[1].pairs[ja1 + off - jc0];
             }
-#pragma unroll
-            for (uint32_t u = 0; u < kFlatDepth; u++)
-                if (t0 + 32u * u + lane < total) addPair(pr[u], pq[u]);
+            const uint32_t c0 = flat ? b0 - a0 : 0u;
+            const uint32_t cnt = flat ? len : 0u;
+            uint32_t incl = cnt;
+    #pragma unroll
+            for (uint32_t off = 1; off < 32; off <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+                if (lane >= off) incl += v;
+            }
+            const uint32_t excl = incl - cnt;
+            const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            for (uint32_t f0 = 0; f0 < total; f0 += 32u * kFlatDepth) {
+                uint64_t pr[kFlatDepth];
+                float pq[kFlatDepth];
+    #pragma unroll
+                for (uint32_t u = 0; u < kFlatDepth; u++) {
+                    const uint32_t t = f0 + 32u * u + lane;
+                    // owner lane: the last j with excl_j <= t (excl is non-decreasing; it holds pairs)
+                    uint32_t j = 0;
+    #pragma unroll
+                    for (uint32_t step = 16; step > 0; step >>= 1) {
+                        const uint32_t v = __shfl_sync(0xFFFFFFFFu, excl, j + step);
+                        if (v <= t) j += step;
+                    }
+                    const uint32_t off = t - __shfl_sync(0xFFFFFFFFu, excl, j);
+                    const uint32_t jc0 = __shfl_sync(0xFFFFFFFFu, c0, j);
+                    const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), ja1 = __shfl_sync(0xFFFFFFFFu, a1, j);
+                    pq[u] = __shfl_sync(0xFFFFFFFFu, qv, j);
+                    pr[u] = 0;
+                    if (t < total) pr[u] = off < jc0 ? P.seg[0].pairs[ja0 + off] : P.seg[1].pairs[ja1 + off - jc0];
+                }
+    #pragma unroll
+                for (uint32_t u = 0; u < kFlatDepth; u++)
+                    if (f0 + 32u * u + lane < total) addPair(pr[u], pq[u]);
+            }
         }
     }
     __syncthreads();
@@ -704,7 +710,7 @@ struct Segment {
     PoolBuffer pairs;     // u64 slot << 32 | float bits of the leaf-level document entry
     PoolBuffer tf;        // u32 per pair
     uint32_t slotBeg = 0, slotEnd = 0;
-    uint64_t stride = 0;  // nbLeaves when each shard of kSmemDocs slots has its own CSR
+    uint64_t stride = 0;  // nbLeaves when each shard of kShardDocs slots has its own CSR
     uint32_t shardBeg = 0, nShards = 1;
     SegmentView view() const
     {
@@ -712,6 +718,21 @@ struct Segment {
                            nShards};
     }
 };
+
+template <uint32_t kThreads>
+void launchScore(bool sharded, dim3 grid, size_t smem, cudaStream_t stream, const ScoreParams& P)
+{
+    if (sharded) {
+        RBW_CUDA(cudaFuncSetAttribute(scoreKernel<true, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(smem)));
+        scoreKernel<true, kThreads><<<grid, kThreads, smem, stream>>>(P);
+    } else {
+        RBW_CUDA(cudaFuncSetAttribute(scoreKernel<false, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(smem)));
+        scoreKernel<false, kThreads><<<grid, kThreads, smem, stream>>>(P);
+    }
+    RBW_CUDA(cudaGetLastError());
+}
 
 } // namespace
 
@@ -857,7 +878,21 @@ public:
         }
         const uint32_t nDocs = mIndexed;
         cudaMemPool_t pool = libraryPool();
-        const uint32_t shardDocs = std::min(std::max(nDocs, 1u), kSmemDocs);
+        int dev = 0, sms = 0;
+        RBW_CUDA(cudaGetDevice(&dev));
+        RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        // Document range per scoring CTA.  With per-shard inverted files it is csrPerCta shards
+        // of kShardDocs documents: the most (up to kSmemDocs documents) that still gives two
+        // CTAs per SM, so a small batch spreads over the GPU; with one inverted file per segment,
+        // kSmemDocs documents (every CTA of a query walks the whole list).
+        uint32_t csrPerCta = 1, shardDocs = std::min(std::max(nDocs, 1u), kSmemDocs);
+        if (perShardIndex()) {
+            csrPerCta = kSmemDocs / kShardDocs;
+            while (csrPerCta > 1 &&
+                   uint64_t(nq) * ((nDocs + csrPerCta * kShardDocs - 1) / (csrPerCta * kShardDocs)) < 2ull * sms)
+                csrPerCta /= 2;
+            shardDocs = std::min(std::max(nDocs, 1u), csrPerCta * kShardDocs);
+        }
         const uint32_t shards = std::max(1u, (nDocs + shardDocs - 1) / shardDocs);
         const size_t entBytes = std::max<uint64_t>(totalLeaves, 1) * mL * sizeof(Entry);
         const size_t candBytes = shards > 1 ? size_t(nq) * shards * k * 8 : 16;
@@ -903,6 +938,7 @@ public:
             P.weights = mWeights.as<float>();
             P.seg[0] = mMain.view();
             P.seg[1] = mDelta.view();
+            P.csrPerCta = csrPerCta;
             P.rcpF = mRcpF.as<float>();
             P.slotDoc = mSlotDoc.as<uint32_t>();
             P.nDocs = nDocs;
@@ -914,9 +950,6 @@ public:
             P.selGlobal = k > kMaxK ? static_cast<unsigned long long*>(selG) : nullptr;
             P.selStride = selStride;
             // more queries than one wave of scoring CTAs: start the longest ones first
-            int dev = 0, sms = 0;
-            RBW_CUDA(cudaGetDevice(&dev));
-            RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             if (nq > uint32_t(sms) && nq <= kOrderMax) {
                 workOrderKernel<<<1, 1024, 0, stream>>>(work, nq, order);
                 RBW_CUDA(cudaGetLastError());
@@ -926,14 +959,16 @@ public:
             P.outScores = dScores;
             P.outCount = dCount;
             const size_t smem = size_t(shardDocs) * 9;
-            if (shards > 1) {
-                RBW_CUDA(cudaFuncSetAttribute(scoreKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-                scoreKernel<true><<<dim3(nq, shards), kScoreThreads, smem, stream>>>(P);
+            // threads per CTA with its documents: 256 up to 2,560, 512 up to 10,240, else 1024
+            const uint32_t threads = shardDocs <= kShardDocs ? 256u : shardDocs <= 4 * kShardDocs ? 512u : 1024u;
+            const dim3 grid(nq, shards);
+            if (threads == 256) {
+                launchScore<256>(shards > 1, grid, smem, stream, P);
+            } else if (threads == 512) {
+                launchScore<512>(shards > 1, grid, smem, stream, P);
             } else {
-                RBW_CUDA(cudaFuncSetAttribute(scoreKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-                scoreKernel<false><<<nq, kScoreThreads, smem, stream>>>(P);
+                launchScore<1024>(shards > 1, grid, smem, stream, P);
             }
-            RBW_CUDA(cudaGetLastError());
             if (shards > 1) {
                 mergeKernel<<<nq, kScoreThreads, 0, stream>>>(P, shards);
                 RBW_CUDA(cudaGetLastError());
@@ -1083,11 +1118,13 @@ private:
         RBW_CUDA(cudaEventRecord(it->second, stream));
     }
 
+    // How a segment's inverted file is laid out: one CSR per shard of kShardDocs documents (each
+    // scoring CTA then reads only its shards' postings), one CSR for the segment, or per shard
+    // while those tables stay small next to the postings themselves.
+    enum class SegLayout { kAuto, kPerShard, kSingle };
+
     // CSR of the documents [s0, s1) into `sg`; their per-leaf posting counts into leafPost.
-    // Documents spanning several shards of kSmemDocs slots get one CSR per shard (each scoring
-    // CTA then reads only its shard's postings) while those tables stay small next to the
-    // postings themselves; otherwise one CSR that every CTA of a query filters.
-    void buildSegment(Segment& sg, uint32_t s0, uint32_t s1, unsigned long long* leafPost)
+    void buildSegment(Segment& sg, uint32_t s0, uint32_t s1, unsigned long long* leafPost, SegLayout layout)
     {
         const uint64_t pairsUpper = mHostDocOff[s1] - mHostDocOff[s0];
         if (pairsUpper >= 0xFFFFFFFFull) throw Error(kUnsupported, "more than 2^32 postings in one segment");
@@ -1096,12 +1133,12 @@ private:
         sg.stride = 0;
         sg.shardBeg = 0;
         sg.nShards = 1;
-        if (s1 > s0) {
-            const uint32_t first = s0 / kSmemDocs, last = (s1 - 1) / kSmemDocs;
+        if (s1 > s0 && layout != SegLayout::kSingle) {
+            const uint32_t first = s0 / kShardDocs, last = (s1 - 1) / kShardDocs;
             const uint64_t tableBytes = (uint64_t(last - first + 1) * mNbLeaves + 1) * 4;
+            const bool small = tableBytes <= std::max<uint64_t>(kShardTableMinBytes, pairsUpper * 12);
             const bool allowed = tunedValue(kTuneDbShardTables, mB, mL, s1 - s0) == 1;
-            if (allowed && last > first &&
-                tableBytes <= std::max<uint64_t>(kShardTableMinBytes, pairsUpper * 12)) {
+            if (layout == SegLayout::kPerShard || (allowed && small)) {
                 sg.stride = mNbLeaves;
                 sg.shardBeg = first;
                 sg.nShards = last - first + 1;
@@ -1206,14 +1243,17 @@ private:
         unsigned long long* leafWords = mWordPost.as<unsigned long long>() + levelBeg(mB, mL - 1) * mB;
         const uint32_t mainEnd = mMain.slotEnd;
         if (s1 - mainEnd > std::max(kDeltaMinDocs, mainEnd / kDeltaFraction)) {
-            buildSegment(mMain, 0, s1, mMainLeafPost.as<unsigned long long>());
-            buildSegment(mDelta, s1, s1, leafWords);
+            buildSegment(mMain, 0, s1, mMainLeafPost.as<unsigned long long>(), SegLayout::kAuto);
+            buildSegment(mDelta, s1, s1, leafWords, SegLayout::kAuto);
             RBW_CUDA(cudaMemcpyAsync(leafWords, mMainLeafPost.get(), mNbLeaves * 8, cudaMemcpyDeviceToDevice,
                                      mStream));
         } else {
             void* deltaPost = nullptr;
             RBW_CUDA(cudaMallocFromPoolAsync(&deltaPost, mNbLeaves * 8, libraryPool(), mStream));
-            buildSegment(mDelta, mainEnd, s1, static_cast<unsigned long long*>(deltaPost));
+            // the delta follows the main segment's layout, so a scoring CTA sees one kind
+            const SegLayout layout = mainEnd == 0 ? SegLayout::kAuto
+                                     : mMain.stride != 0 ? SegLayout::kPerShard : SegLayout::kSingle;
+            buildSegment(mDelta, mainEnd, s1, static_cast<unsigned long long*>(deltaPost), layout);
             leafPostCombine<<<blocks(mNbLeaves, 256), 256, 0, mStream>>>(
                 mMainLeafPost.as<unsigned long long>(), static_cast<unsigned long long*>(deltaPost), leafWords,
                 mNbLeaves);
@@ -1227,6 +1267,13 @@ private:
         RBW_CUDA(cudaGetLastError());
         RBW_CUDA(cudaEventRecord(mIndexReady, mStream));
         mIndexed = s1;
+    }
+
+    // Every segment holding documents has per-shard inverted files (none holds any: false).
+    bool perShardIndex() const
+    {
+        const bool mainDocs = mMain.slotEnd > mMain.slotBeg, deltaDocs = mDelta.slotEnd > mDelta.slotBeg;
+        return (mainDocs || deltaDocs) && (!mainDocs || mMain.stride != 0) && (!deltaDocs || mDelta.stride != 0);
     }
 
     const unsigned long long* skipCounts() const

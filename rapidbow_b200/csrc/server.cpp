@@ -256,14 +256,15 @@ public:
 private:
     // Device bytes a batch of `desc` descriptors in `queries` requests needs: descriptors and
     // leaves, lookup working memory, scoring entries, results and the per-shard candidates of
-    // databases larger than one shard of 20,480 documents, plus 1 MiB of slack.
+    // databases scored by several CTAs per query (at most one per 2,560 documents), plus 1 MiB
+    // of slack.
     size_t estimate(uint64_t desc, uint64_t queries) const
     {
         uint64_t scratch = 0;
         rbw_voc_lookup_scratch_bytes(mVoc, desc, &scratch);
         uint32_t nDocs = 0;
         rbw_db_info(mDb, &nDocs, nullptr);
-        const uint64_t shards = (uint64_t(nDocs) + 20479) / 20480;
+        const uint64_t shards = (uint64_t(nDocs) + 2559) / 2560;
         const uint64_t cand = shards > 1 ? queries * shards * mOpt.max_results * 8ull : 0;
         return size_t(desc * (128 + 4 + 16ull * mLevels) + scratch + queries * (mOpt.max_results * 8ull + 32) + cand +
                       (1u << 20));

@@ -233,9 +233,12 @@ def test_many_documents_use_global_accumulators(oracle):
 
 @pytest.mark.parametrize("layout", [1, 2])
 def test_shard_tables_and_single_table_match_oracle(oracle, layout):
-    """Both inverted-file layouts (one CSR per 20,480-document shard, one CSR for the segment),
-    with a main segment over two shards and a delta segment that straddles a shard boundary;
-    results, postings and upper-level (virtual) inverted files match the oracle."""
+    """Both inverted-file layouts (one CSR per 2,560-document shard, one CSR for the segment),
+    with a main segment over 16 shards and a delta segment that straddles a shard boundary;
+    results, postings and upper-level (virtual) inverted files match the oracle.  Batched
+    queries (scoring CTAs over 1 to 8 shards, by batch size) equal the single queries."""
+    import torch
+
     from rapidbow_b200 import autotune as at
 
     B, L = 16, 3
@@ -264,7 +267,7 @@ def test_shard_tables_and_single_table_match_oracle(oracle, layout):
         for q in qs:
             check_query(db, odb, q, 40)
         assert db.segments() == (n_main, 0)
-        add(n_main, n_main + n_delta)  # slots 39000..41999: shards 1 and 2
+        add(n_main, n_main + n_delta)  # slots 39000..41999: shards 15 and 16
         qs.append(np.concatenate([docs[n_main + 2999], docs[40960]]))
         for q in qs:
             check_query(db, odb, q, 40)
@@ -272,6 +275,18 @@ def test_shard_tables_and_single_table_match_oracle(oracle, layout):
         assert db.segments() == (n_main, n_delta)
         for leaf in {int(docs[0][0]), int(docs[20480][0]), int(docs[n_main + 1500][0]), int(docs[41999][-1])}:
             assert np.array_equal(db.postings(leaf), odb.postings(leaf))
+        for nq in (3, 40, 200):
+            bq = make_queries(docs, B ** L, nq, seed=44 + nq)
+            offs = np.zeros(nq + 1, np.int64)
+            offs[1:] = np.cumsum([q.size for q in bq])
+            bd, bs, bc = db.query_batched(torch.from_numpy(np.concatenate(bq).astype(np.int32)).cuda(),
+                                          torch.from_numpy(offs).cuda(), 30)
+            torch.cuda.synchronize()
+            bd, bs, bc = bd.cpu().numpy().view(np.uint32), bs.cpu().numpy(), bc.cpu().numpy()
+            for i in range(0, nq, max(1, nq // 10)):
+                d, sc = check_query(db, odb, bq[i], 30)
+                assert bc[i] == d.size and np.array_equal(bd[i, : d.size], d)
+                assert np.array_equal(bs[i, : d.size], sc)
     finally:
         at.clear()
 
