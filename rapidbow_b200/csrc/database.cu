@@ -53,7 +53,8 @@ constexpr uint32_t kFlatList = 256;        // leaf lists shorter than this are w
 constexpr uint32_t kFlatDepth = 8;         // pairs per lane in flight in the flattened walk
 constexpr uint32_t kSegThreads = 256;
 constexpr uint32_t kSmemDocs = 20480;     // per-document accumulators kept in shared memory
-constexpr uint32_t kShardDocs = 2560;     // documents per inverted-file shard (kSmemDocs / 8)
+constexpr uint32_t kShardDocs = 2560;     // documents per inverted-file shard
+constexpr uint32_t kGroupShards = kSmemDocs / kShardDocs; // shards per group of kSmemDocs documents (8)
 constexpr uint64_t kShardTableMinBytes = 64ull << 20; // per-shard CSR tables always allowed up to this size
 constexpr uint32_t kMaxK = 1024;          // results selected in shared memory; more in global memory
 constexpr double kFixScale = 72057594037927936.0; // 2^56
@@ -196,25 +197,29 @@ __global__ void __launch_bounds__(kPrepThreads) docPrepKernel(const uint32_t* ne
     if (threadIdx.x == 0) pairCount[slot] = cnt;
 }
 
-// Row of a document's pairs in a segment's offset table: the per-shard CSR of its shard
-// (stride = leaves per shard table), or the single table (stride 0).
-__device__ __forceinline__ uint64_t segRow(uint32_t slot, uint32_t shardBeg, uint64_t stride)
+// Offset-table index of (document slot, leaf) in a segment.  Grouped layout: groups of
+// kSmemDocs documents, then leaves, then the group's kGroupShards shards of kShardDocs
+// documents, so any aligned run of shards of a group holds one leaf's pairs in one range, and a
+// whole group one range per run of leaves.  Single layout (grouped = false): one CSR by leaf.
+__host__ __device__ __forceinline__ uint64_t segIndex(uint32_t slot, uint64_t leaf, uint32_t groupBeg,
+                                                      uint64_t nbLeaves, bool grouped)
 {
-    return stride ? uint64_t(slot / kShardDocs - shardBeg) * stride : 0ull;
+    if (!grouped) return leaf;
+    return ((uint64_t(slot / kSmemDocs - groupBeg) * nbLeaves + leaf) * kGroupShards) +
+           (slot % kSmemDocs) / kShardDocs;
 }
 
-// Per-(shard, leaf) pair counts and per-leaf posting counts of the documents [s0, s0 + gridDim.x).
+// Per-table-entry pair counts and per-leaf posting counts of the documents [s0, s0 + gridDim.x).
 __global__ void segCountKernel(const uint64_t* docOff, const uint64_t* docPairs, const uint32_t* pairCount,
-                               uint32_t s0, uint32_t shardBeg, uint64_t stride, uint32_t* leafPairCnt,
-                               unsigned long long* leafPost)
+                               uint32_t s0, uint32_t groupBeg, uint64_t nbLeaves, bool grouped,
+                               uint32_t* leafPairCnt, unsigned long long* leafPost)
 {
     const uint32_t slot = s0 + blockIdx.x;
     const uint64_t beg = docOff[slot];
-    uint32_t* cnt = leafPairCnt + segRow(slot, shardBeg, stride);
     for (uint32_t p = threadIdx.x; p < pairCount[slot]; p += blockDim.x) {
         const uint64_t v = docPairs[beg + p];
         const uint32_t leaf = static_cast<uint32_t>(v >> 32);
-        atomicAdd(&cnt[leaf], 1u);
+        atomicAdd(&leafPairCnt[segIndex(slot, leaf, groupBeg, nbLeaves, grouped)], 1u);
         atomicAdd(&leafPost[leaf], static_cast<unsigned long long>(static_cast<uint32_t>(v)));
     }
 }
@@ -223,20 +228,20 @@ __global__ void segCountKernel(const uint64_t* docOff, const uint64_t* docPairs,
 // document entry d = tf * w_leaf * rcp (DataBase.cpp:129, the same float products as at query
 // time), tf[] = the raw count for the virtual inverted files of upper levels.
 __global__ void segScatterKernel(const uint64_t* docOff, const uint64_t* docPairs, const uint32_t* pairCount,
-                                 uint32_t s0, uint32_t shardBeg, uint64_t stride, const float* leafWeights,
-                                 const float* rcpF, const uint32_t* leafOff, uint32_t* cursor, uint64_t* pairs,
-                                 uint32_t* tfs)
+                                 uint32_t s0, uint32_t groupBeg, uint64_t nbLeaves, bool grouped,
+                                 const float* leafWeights, const float* rcpF, const uint32_t* leafOff,
+                                 uint32_t* cursor, uint64_t* pairs, uint32_t* tfs)
 {
     const uint32_t slot = s0 + blockIdx.x;
     const uint64_t beg = docOff[slot];
     const float rcp = rcpF[slot];
-    const uint64_t row = segRow(slot, shardBeg, stride);
     for (uint32_t p = threadIdx.x; p < pairCount[slot]; p += blockDim.x) {
         const uint64_t v = docPairs[beg + p];
         const uint32_t leaf = static_cast<uint32_t>(v >> 32);
         const uint32_t tf = static_cast<uint32_t>(v);
         const float d = float(tf) * leafWeights[leaf] * rcp;
-        const uint32_t pos = leafOff[row + leaf] + atomicAdd(&cursor[row + leaf], 1u);
+        const uint64_t idx = segIndex(slot, leaf, groupBeg, nbLeaves, grouped);
+        const uint32_t pos = leafOff[idx] + atomicAdd(&cursor[idx], 1u);
         pairs[pos] = (uint64_t(slot) << 32) | __float_as_uint(d);
         tfs[pos] = tf;
     }
@@ -351,11 +356,11 @@ __global__ void __launch_bounds__(1024) workOrderKernel(const unsigned long long
 }
 
 struct SegmentView {
-    const uint32_t* leafOff;   // [nShards * stride + 1], or [nbLeaves + 1] when stride = 0
+    const uint32_t* leafOff;   // grouped: [nGroups][nbLeaves][kGroupShards] + 1; else [nbLeaves + 1]
     const uint64_t* pairs;     // slot << 32 | float bits of the leaf-level document entry
     const uint32_t* tf;        // descriptors of the document under the leaf
-    uint64_t stride;           // nbLeaves: one CSR per shard of kShardDocs slots; 0: one CSR
-    uint32_t shardBeg, nShards;
+    uint32_t grouped;          // layout (segIndex)
+    uint32_t groupBeg, nGroups;
 };
 
 struct ScoreParams {
@@ -365,7 +370,8 @@ struct ScoreParams {
     const float* qRcpF;
     const float* weights;
     SegmentView seg[2];        // main, delta
-    uint32_t csrPerCta;        // inverted-file shards per CTA (segments with per-shard CSRs), else 1
+    uint32_t csrPerCta;        // shards of kShardDocs documents per CTA (grouped segments)
+    uint64_t nbLeaves;
     const float* rcpF;
     const uint32_t* slotDoc;
     uint32_t nDocs;
@@ -468,10 +474,11 @@ __device__ __forceinline__ void writeResults(const ScoreParams& P, uint32_t q, c
 }
 
 // One CTA per (query, range of shardDocs documents).  The accumulators of the range live in
-// shared memory (9 B per document).  Segments indexed per shard of kShardDocs documents hand
-// the CTA the postings of its csrPerCta shards only; a segment with one inverted file (stride 0)
-// is walked by every CTA of the query, each keeping the postings of its range.  kSharded =
-// false: one range holds every document and no posting needs the range test.
+// shared memory (9 B per document).  Grouped segments hand the CTA the leaf postings of its
+// csrPerCta shards only (one range per leaf word); upper-level words read their group's range
+// and keep the CTA's documents.  A single-layout segment is walked by every CTA of the query,
+// each keeping the postings of its range.  kSharded = false: one range holds every document and
+// no posting needs the range test.
 template <bool kSharded, uint32_t kThreads>
 __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThreads) scoreKernel(ScoreParams P)
 {
@@ -498,12 +505,28 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
     const Entry* ent = P.entries + (P.qOff[q] - P.qOff[0]) * P.L;
     const uint32_t ne = P.entryCount[q];
     const float qRcp = P.qRcpF[q];
-    // Offset table of inverted-file shard `csr` in segment s (nullptr: the segment holds none of
-    // its documents); a one-table segment is walked once, as sub-table 0.
-    auto subTable = [&](int s, uint32_t sub) -> const uint32_t* {
-        if (P.seg[s].stride == 0) return sub == 0 ? P.seg[s].leafOff : nullptr;
-        const uint32_t rel = shard * P.csrPerCta + sub - P.seg[s].shardBeg;
-        return rel < P.seg[s].nShards ? P.seg[s].leafOff + uint64_t(rel) * P.seg[s].stride : nullptr;
+    // The CTA's pair range of a word (leaves [lo, hi)) in segment s.
+    const uint32_t groupOf = docBeg / kSmemDocs, shardInGroup = (docBeg % kSmemDocs) / kShardDocs;
+    auto wordRange = [&](int s, uint64_t lo, uint64_t hi, bool leafLevel, uint32_t& a, uint32_t& b) {
+        const SegmentView& v = P.seg[s];
+        if (!v.grouped) {
+            a = v.leafOff[lo];
+            b = v.leafOff[hi];
+            return;
+        }
+        const uint32_t g = groupOf - v.groupBeg;
+        if (g >= v.nGroups) {
+            a = b = 0;
+            return;
+        }
+        const uint32_t* t = v.leafOff + uint64_t(g) * P.nbLeaves * kGroupShards;
+        if (leafLevel) {
+            a = t[lo * kGroupShards + shardInGroup];
+            b = t[lo * kGroupShards + shardInGroup + P.csrPerCta];
+        } else {
+            a = t[lo * kGroupShards];
+            b = t[hi * kGroupShards];
+        }
     };
     auto addPair = [&](uint64_t pr, float qv) {
         const uint32_t i = static_cast<uint32_t>(pr >> 32) - docBeg;
@@ -550,77 +573,65 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
         const bool valid = e < ne;
         float qv = 0.f, w = 0.f;
         bool leaf = false;
-        uint64_t lo = 0, hi = 0; // the word's leaf range
+        uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
         if (valid) {
             const Entry en = ent[e];
             w = P.weights[en.widx];
             qv = float(en.run) * w * qRcp;
             leaf = en.level == P.L - 1;
             const uint64_t span = ipowDev(P.B, P.L - 1 - en.level);
-            lo = uint64_t(en.word) * span;
-            hi = lo + span;
+            const uint64_t lo = uint64_t(en.word) * span;
+            wordRange(0, lo, lo + span, leaf, a0, b0);
+            wordRange(1, lo, lo + span, leaf, a1, b1);
         }
-        for (uint32_t sub = 0; sub < P.csrPerCta; sub++) {
-            uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
-            const uint32_t* t0 = subTable(0, sub);
-            const uint32_t* t1 = subTable(1, sub);
-            if (valid && t0 != nullptr) {
-                a0 = t0[lo];
-                b0 = t0[hi];
+        const uint32_t len = (b0 - a0) + (b1 - a1);
+        const bool flat = valid && leaf && len < kFlatList;
+        for (uint32_t one = __ballot_sync(0xFFFFFFFFu, valid && !flat); one != 0; one &= one - 1) {
+            const uint32_t j = __ffs(one) - 1;
+            const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), jb0 = __shfl_sync(0xFFFFFFFFu, b0, j);
+            const uint32_t ja1 = __shfl_sync(0xFFFFFFFFu, a1, j), jb1 = __shfl_sync(0xFFFFFFFFu, b1, j);
+            const float jq = __shfl_sync(0xFFFFFFFFu, qv, j), jw = __shfl_sync(0xFFFFFFFFu, w, j);
+            if (__shfl_sync(0xFFFFFFFFu, leaf, j)) {
+                leafList(P.seg[0].pairs, ja0, jb0, jq);
+                leafList(P.seg[1].pairs, ja1, jb1, jq);
+            } else {
+                virtualList(0, ja0, jb0, jw, jq);
+                virtualList(1, ja1, jb1, jw, jq);
             }
-            if (valid && t1 != nullptr) {
-                a1 = t1[lo];
-                b1 = t1[hi];
-            }
-            const uint32_t len = (b0 - a0) + (b1 - a1);
-            const bool flat = valid && leaf && len < kFlatList;
-            for (uint32_t one = __ballot_sync(0xFFFFFFFFu, valid && !flat); one != 0; one &= one - 1) {
-                const uint32_t j = __ffs(one) - 1;
-                const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), jb0 = __shfl_sync(0xFFFFFFFFu, b0, j);
-                const uint32_t ja1 = __shfl_sync(0xFFFFFFFFu, a1, j), jb1 = __shfl_sync(0xFFFFFFFFu, b1, j);
-                const float jq = __shfl_sync(0xFFFFFFFFu, qv, j), jw = __shfl_sync(0xFFFFFFFFu, w, j);
-                if (__shfl_sync(0xFFFFFFFFu, leaf, j)) {
-                    leafList(P.seg[0].pairs, ja0, jb0, jq);
-                    leafList(P.seg[1].pairs, ja1, jb1, jq);
-                } else {
-                    virtualList(0, ja0, jb0, jw, jq);
-                    virtualList(1, ja1, jb1, jw, jq);
+        }
+        const uint32_t c0 = flat ? b0 - a0 : 0u;
+        const uint32_t cnt = flat ? len : 0u;
+        uint32_t incl = cnt;
+#pragma unroll
+        for (uint32_t off = 1; off < 32; off <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+            if (lane >= off) incl += v;
+        }
+        const uint32_t excl = incl - cnt;
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        for (uint32_t f0 = 0; f0 < total; f0 += 32u * kFlatDepth) {
+            uint64_t pr[kFlatDepth];
+            float pq[kFlatDepth];
+#pragma unroll
+            for (uint32_t u = 0; u < kFlatDepth; u++) {
+                const uint32_t t = f0 + 32u * u + lane;
+                // owner lane: the last j with excl_j <= t (excl is non-decreasing; it holds pairs)
+                uint32_t j = 0;
+#pragma unroll
+                for (uint32_t step = 16; step > 0; step >>= 1) {
+                    const uint32_t v = __shfl_sync(0xFFFFFFFFu, excl, j + step);
+                    if (v <= t) j += step;
                 }
+                const uint32_t off = t - __shfl_sync(0xFFFFFFFFu, excl, j);
+                const uint32_t jc0 = __shfl_sync(0xFFFFFFFFu, c0, j);
+                const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), ja1 = __shfl_sync(0xFFFFFFFFu, a1, j);
+                pq[u] = __shfl_sync(0xFFFFFFFFu, qv, j);
+                pr[u] = 0;
+                if (t < total) pr[u] = off < jc0 ? P.seg[0].pairs[ja0 + off] : P.seg[1].pairs[ja1 + off - jc0];
             }
-            const uint32_t c0 = flat ? b0 - a0 : 0u;
-            const uint32_t cnt = flat ? len : 0u;
-            uint32_t incl = cnt;
-    #pragma unroll
-            for (uint32_t off = 1; off < 32; off <<= 1) {
-                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
-                if (lane >= off) incl += v;
-            }
-            const uint32_t excl = incl - cnt;
-            const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-            for (uint32_t f0 = 0; f0 < total; f0 += 32u * kFlatDepth) {
-                uint64_t pr[kFlatDepth];
-                float pq[kFlatDepth];
-    #pragma unroll
-                for (uint32_t u = 0; u < kFlatDepth; u++) {
-                    const uint32_t t = f0 + 32u * u + lane;
-                    // owner lane: the last j with excl_j <= t (excl is non-decreasing; it holds pairs)
-                    uint32_t j = 0;
-    #pragma unroll
-                    for (uint32_t step = 16; step > 0; step >>= 1) {
-                        const uint32_t v = __shfl_sync(0xFFFFFFFFu, excl, j + step);
-                        if (v <= t) j += step;
-                    }
-                    const uint32_t off = t - __shfl_sync(0xFFFFFFFFu, excl, j);
-                    const uint32_t jc0 = __shfl_sync(0xFFFFFFFFu, c0, j);
-                    const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), ja1 = __shfl_sync(0xFFFFFFFFu, a1, j);
-                    pq[u] = __shfl_sync(0xFFFFFFFFu, qv, j);
-                    pr[u] = 0;
-                    if (t < total) pr[u] = off < jc0 ? P.seg[0].pairs[ja0 + off] : P.seg[1].pairs[ja1 + off - jc0];
-                }
-    #pragma unroll
-                for (uint32_t u = 0; u < kFlatDepth; u++)
-                    if (f0 + 32u * u + lane < total) addPair(pr[u], pq[u]);
-            }
+#pragma unroll
+            for (uint32_t u = 0; u < kFlatDepth; u++)
+                if (f0 + 32u * u + lane < total) addPair(pr[u], pq[u]);
         }
     }
     __syncthreads();
@@ -706,16 +717,16 @@ private:
 };
 
 struct Segment {
-    PoolBuffer leafOff;   // u32 [nShards * stride + 1]; [nbLeaves + 1] when stride = 0
+    PoolBuffer leafOff;   // u32 offset table (segIndex) + 1 tail entry
     PoolBuffer pairs;     // u64 slot << 32 | float bits of the leaf-level document entry
     PoolBuffer tf;        // u32 per pair
     uint32_t slotBeg = 0, slotEnd = 0;
-    uint64_t stride = 0;  // nbLeaves when each shard of kShardDocs slots has its own CSR
-    uint32_t shardBeg = 0, nShards = 1;
+    bool grouped = false; // grouped layout: groups of kSmemDocs documents, leaves, shards
+    uint32_t groupBeg = 0, nGroups = 1;
     SegmentView view() const
     {
-        return SegmentView{leafOff.as<uint32_t>(), pairs.as<uint64_t>(), tf.as<uint32_t>(), stride, shardBeg,
-                           nShards};
+        return SegmentView{leafOff.as<uint32_t>(), pairs.as<uint64_t>(), tf.as<uint32_t>(), grouped ? 1u : 0u,
+                           groupBeg, nGroups};
     }
 };
 
@@ -881,12 +892,12 @@ public:
         int dev = 0, sms = 0;
         RBW_CUDA(cudaGetDevice(&dev));
         RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        // Document range per scoring CTA.  With per-shard inverted files it is csrPerCta shards
-        // of kShardDocs documents: the most (up to kSmemDocs documents) that still gives two
-        // CTAs per SM, so a small batch spreads over the GPU; with one inverted file per segment,
-        // kSmemDocs documents (every CTA of a query walks the whole list).
+        // Document range per scoring CTA.  With grouped inverted files it is csrPerCta shards of
+        // kShardDocs documents: the most (up to a group of kSmemDocs documents) that still gives
+        // two CTAs per SM, so a small batch spreads over the GPU; with one inverted file per
+        // segment, kSmemDocs documents (every CTA of a query walks the whole list).
         uint32_t csrPerCta = 1, shardDocs = std::min(std::max(nDocs, 1u), kSmemDocs);
-        if (perShardIndex()) {
+        if (groupedIndex()) {
             csrPerCta = kSmemDocs / kShardDocs;
             while (csrPerCta > 1 &&
                    uint64_t(nq) * ((nDocs + csrPerCta * kShardDocs - 1) / (csrPerCta * kShardDocs)) < 2ull * sms)
@@ -939,6 +950,7 @@ public:
             P.seg[0] = mMain.view();
             P.seg[1] = mDelta.view();
             P.csrPerCta = csrPerCta;
+            P.nbLeaves = mNbLeaves;
             P.rcpF = mRcpF.as<float>();
             P.slotDoc = mSlotDoc.as<uint32_t>();
             P.nDocs = nDocs;
@@ -1053,13 +1065,17 @@ public:
         updateIndex();
         std::shared_lock<std::shared_mutex> lk(mMu);
         std::vector<uint32_t> out;
-        std::vector<std::pair<const Segment*, uint32_t>> tables; // (segment, shard table)
+        std::vector<std::pair<const Segment*, uint32_t>> groups; // (segment, group)
         for (const Segment* sg : {&mMain, &mDelta})
-            for (uint32_t sh = 0; sh < sg->nShards; sh++) tables.emplace_back(sg, sh);
-        for (const auto& [sg, sh] : tables) {
+            for (uint32_t g = 0; g < sg->nGroups; g++) groups.emplace_back(sg, g);
+        for (const auto& [sg, g] : groups) {
+            // the leaf's pairs of the whole group: [index(leaf, shard 0), index(leaf + 1, shard 0))
+            const uint32_t slot = (sg->groupBeg + g) * kSmemDocs;
+            const uint64_t i0 = segIndex(slot, leaf, sg->groupBeg, mNbLeaves, sg->grouped);
+            const uint64_t i1 = segIndex(slot, uint64_t(leaf) + 1, sg->groupBeg, mNbLeaves, sg->grouped);
             uint32_t ab[2] = {0, 0};
-            RBW_CUDA(cudaMemcpyAsync(ab, sg->leafOff.as<uint32_t>() + sh * sg->stride + leaf, 8,
-                                     cudaMemcpyDeviceToHost, mStream));
+            RBW_CUDA(cudaMemcpyAsync(&ab[0], sg->leafOff.as<uint32_t>() + i0, 4, cudaMemcpyDeviceToHost, mStream));
+            RBW_CUDA(cudaMemcpyAsync(&ab[1], sg->leafOff.as<uint32_t>() + i1, 4, cudaMemcpyDeviceToHost, mStream));
             RBW_CUDA(cudaStreamSynchronize(mStream));
             if (ab[1] < ab[0]) throw Error(kInternal, "inconsistent posting offsets");
             std::vector<uint64_t> pr(ab[1] - ab[0]);
@@ -1118,10 +1134,10 @@ private:
         RBW_CUDA(cudaEventRecord(it->second, stream));
     }
 
-    // How a segment's inverted file is laid out: one CSR per shard of kShardDocs documents (each
-    // scoring CTA then reads only its shards' postings), one CSR for the segment, or per shard
-    // while those tables stay small next to the postings themselves.
-    enum class SegLayout { kAuto, kPerShard, kSingle };
+    // How a segment's inverted file is laid out: grouped (segIndex; each scoring CTA then reads
+    // only its shards' leaf postings), one CSR for the segment, or grouped while those tables
+    // stay small next to the postings themselves.
+    enum class SegLayout { kAuto, kGrouped, kSingle };
 
     // CSR of the documents [s0, s1) into `sg`; their per-leaf posting counts into leafPost.
     void buildSegment(Segment& sg, uint32_t s0, uint32_t s1, unsigned long long* leafPost, SegLayout layout)
@@ -1130,21 +1146,21 @@ private:
         if (pairsUpper >= 0xFFFFFFFFull) throw Error(kUnsupported, "more than 2^32 postings in one segment");
         sg.slotBeg = s0;
         sg.slotEnd = s1;
-        sg.stride = 0;
-        sg.shardBeg = 0;
-        sg.nShards = 1;
+        sg.grouped = false;
+        sg.groupBeg = 0;
+        sg.nGroups = 1;
         if (s1 > s0 && layout != SegLayout::kSingle) {
-            const uint32_t first = s0 / kShardDocs, last = (s1 - 1) / kShardDocs;
-            const uint64_t tableBytes = (uint64_t(last - first + 1) * mNbLeaves + 1) * 4;
+            const uint32_t first = s0 / kSmemDocs, last = (s1 - 1) / kSmemDocs;
+            const uint64_t tableBytes = (uint64_t(last - first + 1) * mNbLeaves * kGroupShards + 1) * 4;
             const bool small = tableBytes <= std::max<uint64_t>(kShardTableMinBytes, pairsUpper * 12);
             const bool allowed = tunedValue(kTuneDbShardTables, mB, mL, s1 - s0) == 1;
-            if (layout == SegLayout::kPerShard || (allowed && small)) {
-                sg.stride = mNbLeaves;
-                sg.shardBeg = first;
-                sg.nShards = last - first + 1;
+            if (layout == SegLayout::kGrouped || (allowed && small)) {
+                sg.grouped = true;
+                sg.groupBeg = first;
+                sg.nGroups = last - first + 1;
             }
         }
-        const uint64_t entries = uint64_t(sg.nShards) * mNbLeaves;
+        const uint64_t entries = sg.grouped ? uint64_t(sg.nGroups) * mNbLeaves * kGroupShards : mNbLeaves;
         sg.leafOff.reserve((entries + 1) * 4, 0, mStream);
         sg.pairs.reserve(std::max<uint64_t>(pairsUpper, 1) * 8, 0, mStream);
         sg.tf.reserve(std::max<uint64_t>(pairsUpper, 1) * 4, 0, mStream);
@@ -1159,8 +1175,8 @@ private:
         RBW_CUDA(cudaMemsetAsync(leafPost, 0, mNbLeaves * 8, mStream));
         if (s1 > s0) {
             segCountKernel<<<s1 - s0, kSegThreads, 0, mStream>>>(mDocOff.as<uint64_t>(), mDocPairs.as<uint64_t>(),
-                                                                mPairCount.as<uint32_t>(), s0, sg.shardBeg,
-                                                                sg.stride, leafPairCnt, leafPost);
+                                                                mPairCount.as<uint32_t>(), s0, sg.groupBeg,
+                                                                mNbLeaves, sg.grouped, leafPairCnt, leafPost);
             RBW_CUDA(cudaGetLastError());
         }
         uint32_t* leafOff = sg.leafOff.as<uint32_t>();
@@ -1168,8 +1184,9 @@ private:
         leafOffTail<<<1, 1, 0, mStream>>>(leafPairCnt, leafOff, entries);
         if (s1 > s0) {
             segScatterKernel<<<s1 - s0, kSegThreads, 0, mStream>>>(
-                mDocOff.as<uint64_t>(), mDocPairs.as<uint64_t>(), mPairCount.as<uint32_t>(), s0, sg.shardBeg,
-                sg.stride, mWeights.as<float>() + levelBeg(mB, mL - 1) * mB, mRcpF.as<float>(), leafOff, cursor,
+                mDocOff.as<uint64_t>(), mDocPairs.as<uint64_t>(), mPairCount.as<uint32_t>(), s0, sg.groupBeg,
+                mNbLeaves, sg.grouped, mWeights.as<float>() + levelBeg(mB, mL - 1) * mB, mRcpF.as<float>(), leafOff,
+                cursor,
                 sg.pairs.as<uint64_t>(), sg.tf.as<uint32_t>());
         }
         RBW_CUDA(cudaGetLastError());
@@ -1252,7 +1269,7 @@ private:
             RBW_CUDA(cudaMallocFromPoolAsync(&deltaPost, mNbLeaves * 8, libraryPool(), mStream));
             // the delta follows the main segment's layout, so a scoring CTA sees one kind
             const SegLayout layout = mainEnd == 0 ? SegLayout::kAuto
-                                     : mMain.stride != 0 ? SegLayout::kPerShard : SegLayout::kSingle;
+                                     : mMain.grouped ? SegLayout::kGrouped : SegLayout::kSingle;
             buildSegment(mDelta, mainEnd, s1, static_cast<unsigned long long*>(deltaPost), layout);
             leafPostCombine<<<blocks(mNbLeaves, 256), 256, 0, mStream>>>(
                 mMainLeafPost.as<unsigned long long>(), static_cast<unsigned long long*>(deltaPost), leafWords,
@@ -1269,11 +1286,11 @@ private:
         mIndexed = s1;
     }
 
-    // Every segment holding documents has per-shard inverted files (none holds any: false).
-    bool perShardIndex() const
+    // Every segment holding documents has the grouped layout (none holds any: false).
+    bool groupedIndex() const
     {
         const bool mainDocs = mMain.slotEnd > mMain.slotBeg, deltaDocs = mDelta.slotEnd > mDelta.slotBeg;
-        return (mainDocs || deltaDocs) && (!mainDocs || mMain.stride != 0) && (!deltaDocs || mDelta.stride != 0);
+        return (mainDocs || deltaDocs) && (!mainDocs || mMain.grouped) && (!deltaDocs || mDelta.grouped);
     }
 
     const unsigned long long* skipCounts() const

@@ -38,6 +38,7 @@ constexpr uint32_t kBBlockBytes = kNodeBytes * 17;    // node + up to 16 childre
 constexpr uint32_t kTeamWarps = 4;                    // epilogue team: one warp per TMEM lane quarter
 constexpr uint32_t kIssuer1Warp = 2 + 2 * kTeamWarps;        // second MMA issuer, after the teams
 constexpr uint32_t kTcThreads = 32 * (3 + 2 * kTeamWarps); // TMA, two MMA issuers, two epilogue teams
+constexpr uint32_t kRingThreads = kTcThreads + 32;          // ring schedule: three MMA issuers
 constexpr uint32_t kSmemHistMax = 1024;
 constexpr uint32_t kRegroupCtas = 148;                // regroup kernels' CTAs (one per SM on 148 SMs)
 // Two accumulator buffers of 256 columns; tile t uses buffer t & 1.  Its level-2p MMA (16
@@ -669,16 +670,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
 }
 
-// Ring schedule.  One thread issues every MMA in tile order: the node-level MMA of tile t into
-// node entry t % kNodeEntries, then the tile's children in halves (children [0, c0) and
-// [c0, B), c0 = ceil(B / 2), one half when B <= 8) into ring slots n % kRingSlots, n = the
-// running half index.  No children MMA waits for a node-level read: the children accumulators
-// never share columns with the node level, so the tensor pipe runs the halves back to back
-// while the teams read earlier slots.  Half n waits only until half n - kRingSlots has been
-// read; node entry t until tile t - kNodeEntries's entry has been read.  Team t & 1 reads the
-// node level, picks the branch b, then reads the halves (64-column loads) and keeps the 16
-// columns of child b.
-__global__ void __launch_bounds__(kTcThreads, 1)
+// Ring schedule.  Three threads issue the MMAs, each in tile order: warp 1 the node-level MMA
+// of tile t into node entry t % kNodeEntries; warps 10 and 11 the tile's children in halves
+// (children [0, c0) and [c0, B), c0 = ceil(B / 2); one half when B <= 8) into ring slots
+// n % kRingSlots, n = the running half index.  No children MMA waits for a node-level read:
+// the children accumulators never share columns with the node level, so the tensor pipe runs
+// the halves back to back while the teams read earlier slots.  Half n waits only until half
+// n - kRingSlots has been read; node entry t until tile t - kNodeEntries's entry has been read.
+// Team t & 1 reads the node level, picks the branch b, then reads the halves (64-column loads)
+// and keeps the 16 columns of child b.  Every issuer commits its own MMAs (a commit tracks the
+// committing thread's MMAs only) to the tile's stage and the group's centre block barriers.
+__global__ void __launch_bounds__(kRingThreads, 1)
     lookupPassRing(const __grid_constant__ CUtensorMap tmapTile, const PassParams p)
 {
     extern __shared__ uint8_t smemRaw[];
@@ -694,16 +696,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const bool two = p.twoLevels != 0;
     const uint32_t nh = two ? (p.B > 8 ? 2u : 1u) : 0u;   // children halves per tile
     const uint32_t c0 = nh == 2 ? (p.B + 1) / 2 : p.B;     // children in the first half
+    const uint32_t issuers = 1 + nh;
     volatile uint32_t* abortFlag = &S.abortFlag;
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < kStages; s++) {
             mbarInit(&S.aFull[s], 1);
-            mbarInit(&S.aEmpty[s], 1);
+            mbarInit(&S.aEmpty[s], issuers);
         }
         for (uint32_t j = 0; j < 2; j++) {
             mbarInit(&S.bFull[j], 1);
-            mbarInit(&S.bEmpty[j], 1 + 2 * kTeamWarps); // the issuer + both epilogue teams
+            mbarInit(&S.bEmpty[j], issuers + 2 * kTeamWarps); // the issuers + both epilogue teams
         }
         for (uint32_t e = 0; e < kNodeEntries; e++) {
             mbarInit(&S.nodeAcc[e], 1);
@@ -713,7 +716,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mbarInit(&S.slotFull[k], 1);
             mbarInit(&S.slotFree[k], kTeamWarps);
         }
-        mbarInit(&S.mmaDone, 1);
+        mbarInit(&S.mmaDone, issuers);
         S.abortFlag = 0;
         fenceMbarInit();
     }
@@ -732,15 +735,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     tcFenceAfter();
     const uint32_t tmem = S.tmemBase;
+    // issuer role: 0 node level (warp 1), 1 + h children half h (warps 10 and 11)
+    const uint32_t role = warp == 1 ? 0u : warp == kIssuer1Warp ? 1u : warp == kIssuer1Warp + 1 ? 2u : 99u;
     if (nT > 0 && warp == 0) {
         passProducer(S, p, &tmapTile, t0, nT, lane, abortFlag);
-    } else if (nT > 0 && warp == 1) {
-        // ------------------------------------------------------------ MMA issuer (one thread)
+    } else if (nT > 0 && role < issuers) {
+        // ------------------------------------------------------------ MMA issuers (one thread each)
         if (lane == 0) {
-            const uint32_t idescNode = idescU8(16);
+            const uint32_t h = role - 1u;                    // children half (roles 1, 2)
+            const uint32_t cb = h ? c0 : 0u;
+            const uint32_t cnt = h ? p.B - c0 : c0;
+            const uint32_t idesc = role == 0 ? idescU8(16) : idescU8(16u * cnt);
             uint32_t prevGroup = 0xFFFFFFFFu, slot = 1, uses0 = 0, uses1 = 0;
-            bool ok = true;
-            for (uint32_t t = 0; ok && t < nT; t++) {
+            for (uint32_t t = 0; t < nT; t++) {
                 const TileInfo ti = tileAtSmem(S, p, t0, t);
                 if (ti.group != prevGroup) {
                     slot ^= 1u;
@@ -750,39 +757,36 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
                 const uint32_t s = t % kStages;
                 if (!mbarWait(&S.aFull[s], (t / kStages) & 1u, abortFlag, p.err, 41)) break;
-                const uint32_t e = t % kNodeEntries;
-                if (t >= kNodeEntries && !mbarWait(&S.nodeFree[e], ((t / kNodeEntries) - 1u) & 1u, abortFlag, p.err, 42))
-                    break;
-                tcFenceAfter();
                 const uint32_t aBase = smemAddr(S.a[s]);
                 const uint32_t bBase = smemAddr(S.b[slot]);
+                if (role == 0) {
+                    const uint32_t e = t % kNodeEntries;
+                    if (t >= kNodeEntries &&
+                        !mbarWait(&S.nodeFree[e], ((t / kNodeEntries) - 1u) & 1u, abortFlag, p.err, 42))
+                        break;
+                    tcFenceAfter();
 #pragma unroll
-                for (uint32_t q4 = 0; q4 < 4; q4++) {
-                    mmaU8(tmem + kNodeCol0 + 16u * e, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4),
-                          idescNode, q4 > 0 ? 1u : 0u);
-                }
-                mmaCommit(&S.nodeAcc[e]);
-                for (uint32_t h = 0; h < nh; h++) {
+                    for (uint32_t q4 = 0; q4 < 4; q4++) {
+                        mmaU8(tmem + kNodeCol0 + 16u * e, smemDescSw128(aBase + 32u * q4),
+                              smemDescSw128(bBase + 32u * q4), idesc, q4 > 0 ? 1u : 0u);
+                    }
+                    mmaCommit(&S.nodeAcc[e]);
+                } else {
                     const uint32_t n = t * nh + h;
                     const uint32_t k = n % kRingSlots;
-                    if (n >= kRingSlots && !mbarWait(&S.slotFree[k], ((n / kRingSlots) - 1u) & 1u, abortFlag, p.err, 43)) {
-                        ok = false;
+                    if (n >= kRingSlots &&
+                        !mbarWait(&S.slotFree[k], ((n / kRingSlots) - 1u) & 1u, abortFlag, p.err, 43))
                         break;
-                    }
                     tcFenceAfter();
-                    const uint32_t cb = h ? c0 : 0u;
-                    const uint32_t cnt = h ? p.B - c0 : c0;
-                    const uint32_t idesc = idescU8(16u * cnt);
                     const uint32_t cBase = bBase + kNodeBytes * (1u + cb);
 #pragma unroll
                     for (uint32_t q4 = 0; q4 < 4; q4++) {
-                        mmaU8(tmem + kSlotCols * k, smemDescSw128(aBase + 32u * q4), smemDescSw128(cBase + 32u * q4),
-                              idesc, q4 > 0 ? 1u : 0u);
+                        mmaU8(tmem + kSlotCols * k, smemDescSw128(aBase + 32u * q4),
+                              smemDescSw128(cBase + 32u * q4), idesc, q4 > 0 ? 1u : 0u);
                     }
                     mmaCommit(&S.slotFull[k]);
                 }
-                if (!ok) break;
-                mmaCommit(&S.aEmpty[s]); // the tile's stage is free once its MMAs are done
+                mmaCommit(&S.aEmpty[s]); // the stage is free once every issuer's MMAs on it are done
                 if (lastOfGroupSmem(S, p, t0, nT, t, ti.group)) mmaCommit(&S.bEmpty[slot]);
             }
             mmaCommit(&S.mmaDone);
@@ -1405,7 +1409,7 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
         {
             ScopedKernelTimer timer(kTimedLookupPass, stream);
             if (ring) {
-                lookupPassRing<<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
+                lookupPassRing<<<grid, kRingThreads, kTcSmemBytes, stream>>>(tmapTile, p);
             } else if (warpNode) {
                 lookupPassTc<true><<<grid, kTcThreads, kTcSmemBytes, stream>>>(tmapTile, p);
             } else {

@@ -233,7 +233,7 @@ def test_many_documents_use_global_accumulators(oracle):
 
 @pytest.mark.parametrize("layout", [1, 2])
 def test_shard_tables_and_single_table_match_oracle(oracle, layout):
-    """Both inverted-file layouts (one CSR per 2,560-document shard, one CSR for the segment),
+    """Both inverted-file layouts (grouped tables per 2,560-document shard, one CSR per segment),
     with a main segment over 16 shards and a delta segment that straddles a shard boundary;
     results, postings and upper-level (virtual) inverted files match the oracle.  Batched
     queries (scoring CTAs over 1 to 8 shards, by batch size) equal the single queries."""
