@@ -268,6 +268,7 @@ def run_ours(args, world, rank, local):
         kern = None
         if kernel_name:
             kern = rbw.timing_read(kernel_name)
+            timed.regroup = rbw.timing_read("lookup_regroup")
         return allreduce_max(world, ms), launches, kern
 
     # autotuning (before the timed region): rows per thread of the regroup scatter, on this lookup
@@ -280,6 +281,7 @@ def run_ours(args, world, rank, local):
                  "default_ms": e["default_ms"], "kernel": "scanBins + buildTiles + scatterRows (per lookup)"}
     with ClockSampler(local) as clocks:
         ms, launches, (k_ms, k_n) = timed(args.algo, args.steps, args.warmup, "lookup_pass_tc")
+    regroup_ms, regroup_n = timed.regroup
     clk = clocks.summary()
     ms_simt, _, (s_ms, s_n) = timed("simt_f32", max(3, args.steps // 4), 2, "lookup_simt_f32")
     # exactness on the bench data: tensor-core IDs == FP32 kernel IDs
@@ -310,6 +312,10 @@ def run_ours(args, world, rank, local):
                      "kernel": "lookupPassTc", "launch_ms": k_avg_ms, "launches_per_step": k_n / args.steps,
                      "algorithmic_bytes_per_launch": n * BYTES_PER_DESC},
         "whole_lookup_hbm_frac": (n * BYTES_PER_DESC / (ms / 1e3) / 1e9) / hbm_peak,
+        "regroup": {"ms_per_step": regroup_ms / args.steps, "regroups_per_step": regroup_n / args.steps,
+                    "kernels": "regroupHist + regroupScan + buildTiles + regroupScatter",
+                    "algorithmic_bytes": 8 * n,
+                    "achieved_gbs": 8 * n / (regroup_ms / max(regroup_n, 1) / 1e3) / 1e9 if regroup_n else None},
         "clocks": clk,
         "device_errors": [code, where],
     }

@@ -386,7 +386,8 @@ RBW_API int rbw_tuning_clear(void);
  * counterpart; used by bench.py).  While enabled, each launch of a timed kernel is bracketed by
  * two events on its stream.  rbw_timing_read sums completed launches of one kernel id:
  * 0 lookup tensor pass, 1 lookup FP32 SIMT, 2 lookup regroup, 3 k-means assign,
- * 4 k-means update, 5 scoring, 6 inverted-file construction.  Read after synchronising. */
+ * 4 k-means update, 5 scoring (all of it), 6 inverted-file construction, 7 query preparation
+ * and 8 candidate merge (both also inside 5).  Read after synchronising. */
 RBW_API void rbw_timing_enable(int32_t on);
 RBW_API int rbw_timing_reset(void);
 RBW_API int rbw_timing_read(uint32_t kernel, double* total_ms, uint64_t* launches);

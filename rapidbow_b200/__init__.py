@@ -333,7 +333,7 @@ class Vocabulary:
 
 
 TIMED_KERNELS = {"lookup_pass_tc": 0, "lookup_simt_f32": 1, "lookup_regroup": 2, "kmeans_assign": 3,
-                 "kmeans_update": 4, "score": 5, "index": 6}
+                 "kmeans_update": 4, "score": 5, "index": 6, "score_prep": 7, "score_merge": 8}
 
 
 def timing_enable(on: bool) -> None:

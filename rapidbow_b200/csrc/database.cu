@@ -39,6 +39,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <optional>
 #include <shared_mutex>
 #include <unordered_map>
 #include <vector>
@@ -924,6 +925,7 @@ public:
         RBW_CUDA(cudaMallocFromPoolAsync(&big, bigBytes, pool, stream));
         {
             ScopedKernelTimer timer(kTimedScore, stream);
+            std::optional<ScopedKernelTimer> prepTimer(std::in_place, kTimedScorePrep, stream);
             const size_t prepSmem = size_t(nextPow2(std::max(maxN, 1u))) * 4;
             RBW_CUDA(cudaFuncSetAttribute(queryPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(prepSmem)));
             queryPrepKernel<<<nq, kPrepThreads, prepSmem, stream>>>(
@@ -941,6 +943,7 @@ public:
                     static_cast<uint32_t*>(cnt), work);
                 RBW_CUDA(cudaGetLastError());
             }
+            prepTimer.reset();
             ScoreParams P{};
             P.entries = static_cast<const Entry*>(ent);
             P.entryCount = static_cast<const uint32_t*>(cnt);
@@ -982,6 +985,7 @@ public:
                 launchScore<1024>(shards > 1, grid, smem, stream, P);
             }
             if (shards > 1) {
+                ScopedKernelTimer mergeTimer(kTimedScoreMerge, stream);
                 mergeKernel<<<nq, kScoreThreads, 0, stream>>>(P, shards);
                 RBW_CUDA(cudaGetLastError());
             }

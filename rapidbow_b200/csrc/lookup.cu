@@ -1087,8 +1087,15 @@ __global__ void __launch_bounds__(1024) regroupScan(uint32_t* ctaHist, uint32_t 
     const bool active = k < chunks;
     const uint32_t c0 = active ? k * len : nCta;
     const uint32_t c1 = active ? min(nCta, c0 + len) : nCta;
+    // eight loads in flight per step (the loop is bound by load latency)
     uint32_t sum = 0;
-    for (uint32_t c = c0; c < c1; c++) sum += ctaHist[uint64_t(c) * nb + b];
+    for (uint32_t c = c0; c < c1; c += 8) {
+        uint32_t v[8];
+#pragma unroll
+        for (uint32_t u = 0; u < 8; u++) v[u] = c + u < c1 ? ctaHist[uint64_t(c + u) * nb + b] : 0u;
+#pragma unroll
+        for (uint32_t u = 0; u < 8; u++) sum += v[u];
+    }
     part[tid] = sum;
     __syncthreads();
     // bin totals and the chunk's prefix inside its bin
@@ -1148,11 +1155,15 @@ __global__ void __launch_bounds__(1024) regroupScan(uint32_t* ctaHist, uint32_t 
     __syncthreads();
     if (active) {
         uint32_t run = part[b] + before;
-        for (uint32_t c = c0; c < c1; c++) {
-            const uint64_t i = uint64_t(c) * nb + b;
-            const uint32_t v = ctaHist[i];
-            ctaHist[i] = run;
-            run += v;
+        for (uint32_t c = c0; c < c1; c += 8) {
+            uint32_t v[8];
+#pragma unroll
+            for (uint32_t u = 0; u < 8; u++) v[u] = c + u < c1 ? ctaHist[uint64_t(c + u) * nb + b] : 0u;
+#pragma unroll
+            for (uint32_t u = 0; u < 8; u++) {
+                if (c + u < c1) ctaHist[uint64_t(c + u) * nb + b] = run;
+                run += v[u];
+            }
         }
     }
 }

@@ -13,9 +13,11 @@ enum TimedKernel : uint32_t {
     kTimedRegroup = 2,      // scan + tile list + scatter between lookup passes
     kTimedAssign = 3,       // k-means assign
     kTimedUpdate = 4,       // k-means update
-    kTimedScore = 5,        // inverted-file scoring
+    kTimedScore = 5,        // inverted-file scoring (query preparation, scoring, merge)
     kTimedIndex = 6,        // inverted-file construction
-    kTimedCount = 8,
+    kTimedScorePrep = 7,    // query preparation alone (inside kTimedScore)
+    kTimedScoreMerge = 8,   // merge of the per-CTA candidates alone (inside kTimedScore)
+    kTimedCount = 9,
 };
 
 bool timingEnabled();
