@@ -114,6 +114,18 @@ __device__ void bitonicSortShared(T* keys, uint32_t nPow2)
     }
 }
 
+// Warp-aggregated slot allocation: the warp's lanes with `take` get consecutive slots from
+// *counter (one atomic per warp).  Every lane of the warp must call it.
+__device__ __forceinline__ uint32_t warpSlot(bool take, uint32_t* counter)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t mask = __ballot_sync(0xFFFFFFFFu, take);
+    uint32_t base = 0;
+    if (lane == 0 && mask != 0) base = atomicAdd(counter, uint32_t(__popc(mask)));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
 // Loads n leaf indices, sorts them and returns how many are valid (< nbLeaves): leaves out of
 // range sort to the end and are ignored, so a bad index never reaches a table lookup.
 __device__ uint32_t loadAndSort(const uint32_t* src, uint32_t n, uint32_t* keys, uint64_t nbLeaves, uint32_t* nValid)
@@ -162,6 +174,95 @@ __device__ double l1NormWarp(const uint32_t* sorted, uint32_t n, const float* we
     return norm;
 }
 
+// The same sum by the whole block.  When every term is finite and >= 0, each is an integer
+// multiple of 2^e, e = the lowest set bit of any term; if the exact total is below 2^(e + 53),
+// every partial sum of the reference's order is an exactly representable double, so no
+// addition in that order rounds and the in-order double sum equals the exact total, which the
+// block forms here in any order with 64-bit integers (one pass for e, one for the total).
+// Otherwise warp 0 adds the terms in order (l1NormWarp).  Call from every thread; the result
+// is valid in every thread.
+__device__ double l1NormBlock(const uint32_t* sorted, uint32_t n, const float* weights, uint32_t B, uint32_t L)
+{
+    __shared__ int32_t sLsb;
+    __shared__ uint32_t sBad;
+    __shared__ unsigned long long sTotal;
+    __shared__ double sNorm;
+    if (threadIdx.x == 0) {
+        sLsb = 0x7FFFFFFF;
+        sBad = 0;
+        sTotal = 0;
+    }
+    __syncthreads();
+    // exponent of bit 0 of the significand and the significand (implicit bit included)
+    auto split = [](uint32_t bits, int32_t& e0, uint32_t& m) {
+        const uint32_t ef = (bits >> 23) & 0xFFu;
+        m = (bits & 0x7FFFFFu) | (ef ? 0x800000u : 0u);
+        e0 = int32_t(ef ? ef : 1u) - 150;
+    };
+    int32_t lsb = 0x7FFFFFFF;
+    uint32_t bad = 0;
+    uint32_t span = 1;
+    for (uint32_t it = 0; it < L; it++) {
+        const float* lw = weights + levelBegDev(B, L - 1 - it) * B;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t bits = __float_as_uint(lw[sorted[i] / span]);
+            if ((bits & 0x7FFFFFFFu) == 0) continue; // +-0 adds nothing
+            if ((bits >> 31) != 0 || ((bits >> 23) & 0xFFu) == 0xFFu) {
+                bad = 1;                              // negative, infinite or NaN
+                continue;
+            }
+            int32_t e0;
+            uint32_t m;
+            split(bits, e0, m);
+            lsb = min(lsb, e0 + int32_t(__ffs(m)) - 1);
+        }
+        span *= B;
+    }
+    atomicMin(&sLsb, lsb);
+    if (bad) atomicOr(&sBad, 1u);
+    __syncthreads();
+    const int32_t e = sLsb;
+    if (!sBad && e != 0x7FFFFFFF) {
+        constexpr unsigned long long kLimit = 1ull << 53;
+        unsigned long long total = 0;
+        span = 1;
+        for (uint32_t it = 0; it < L && !bad; it++) {
+            const float* lw = weights + levelBegDev(B, L - 1 - it) * B;
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const uint32_t bits = __float_as_uint(lw[sorted[i] / span]);
+                if ((bits & 0x7FFFFFFFu) == 0) continue;
+                int32_t e0;
+                uint32_t m;
+                split(bits, e0, m);
+                const int32_t shift = e0 - e; // >= 0: e is at most this term's lowest set bit
+                if (shift + 32 - int32_t(__clz(m)) > 53) {
+                    bad = 1;                  // the term alone reaches 2^(e + 53)
+                    break;
+                }
+                total += static_cast<unsigned long long>(m) << shift;
+                if (total >= kLimit) {
+                    bad = 1;
+                    break;
+                }
+            }
+            span *= B;
+        }
+        if (bad) atomicOr(&sBad, 1u);
+        atomicAdd(&sTotal, total);            // < blockDim * 2^53: no overflow
+        __syncthreads();
+        if (!sBad && sTotal < kLimit) return ldexp(static_cast<double>(sTotal), e);
+    } else if (e == 0x7FFFFFFF && !sBad) {
+        return 0.0; // every term is zero
+    }
+    // some partial sum may round: the reference's order, one term after another
+    if (threadIdx.x < 32) {
+        const double norm = l1NormWarp(sorted, n, weights, B, L);
+        if (threadIdx.x == 0) sNorm = norm;
+    }
+    __syncthreads();
+    return sNorm;
+}
+
 // ------------------------------------------------------------------ documents
 // One CTA per new document.  newLeaves holds the new documents' leaves back to back, starting at
 // posting offset docOff[s0].  Without gkeys, CTA i prepares slot s0 + i in shared memory and
@@ -182,16 +283,17 @@ __global__ void __launch_bounds__(kPrepThreads) docPrepKernel(const uint32_t* ne
     uint32_t* keys = gkeys ? gkeys + uint64_t(blockIdx.x) * gstride : skeys;
     if (threadIdx.x == 0) cnt = 0;
     const uint32_t n = loadAndSort(newLeaves + (beg - docOff[s0]), nAll, keys, nbLeaves, &nValid);
-    if (threadIdx.x < 32) {
-        const double norm = l1NormWarp(keys, n, weights, B, L);
-        if (threadIdx.x == 0) rcpF[slot] = float(1 / norm); // DataBase.cpp:68
-    }
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint32_t k = keys[i];
-        if (i == 0 || keys[i - 1] != k) {
+    const double norm = l1NormBlock(keys, n, weights, B, L);
+    if (threadIdx.x == 0) rcpF[slot] = float(1 / norm); // DataBase.cpp:68
+    for (uint32_t base = 0; base < n; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t k = i < n ? keys[i] : 0u;
+        const bool head = i < n && (i == 0 || keys[i - 1] != k);
+        const uint32_t pos = warpSlot(head, &cnt);
+        if (head) {
             uint32_t run = 1;
             while (i + run < n && keys[i + run] == k) run++;
-            docPairs[beg + atomicAdd(&cnt, 1u)] = (uint64_t(k) << 32) | run;
+            docPairs[beg + pos] = (uint64_t(k) << 32) | run;
         }
     }
     __syncthreads();
@@ -299,18 +401,21 @@ __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* 
         workSum = 0;
     }
     const uint32_t n = loadAndSort(qLeaves + beg, nAll, keys, nbLeaves, &nValid);
-    if (threadIdx.x < 32) {
-        const double norm = l1NormWarp(keys, n, weights, B, L);
-        if (threadIdx.x == 0) qRcpF[q] = float(1 / norm); // DataBase.cpp:77-94
-    }
+    const double norm = l1NormBlock(keys, n, weights, B, L);
+    if (threadIdx.x == 0) qRcpF[q] = float(1 / norm); // DataBase.cpp:77-94
     uint32_t span = 1; // B^it; leaf indices are 32-bit, so is every span
     const uint64_t limit = 16ull + 4ull * k; // DataBase.h:60-61, DataBase.cpp:125
+    unsigned long long myWork = 0;            // postings the scoring will read
     for (uint32_t it = 0; it < L; it++) {
         const uint32_t level = L - 1 - it;
         const uint64_t base = levelBegDev(B, level) * B;
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const uint32_t word = keys[i] / span;
-            if (i == 0 || keys[i - 1] / span != word) {
+        for (uint32_t i0 = 0; i0 < n; i0 += blockDim.x) {
+            const uint32_t i = i0 + threadIdx.x;
+            const uint32_t word = i < n ? keys[i] / span : 0u;
+            bool keep = false;
+            uint32_t run = 0;
+            uint64_t widx = 0;
+            if (i < n && (i == 0 || keys[i - 1] / span != word)) {
                 // the run of `word` ends at the first key >= (word + 1) * span (keys are sorted)
                 const uint64_t end = (uint64_t(word) + 1) * span;
                 uint32_t lo = i + 1, hi = n;
@@ -319,17 +424,19 @@ __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* 
                     if (keys[mid] < end) lo = mid + 1;
                     else hi = mid;
                 }
-                const uint32_t run = lo - i;
-                const uint64_t widx = base + word;
-                if (it == 0 || wordPost[widx] < limit) {
-                    const uint32_t p = atomicAdd(&cnt, 1u);
-                    out[p] = Entry{level, word, run, static_cast<uint32_t>(widx)};
-                    atomicAdd(&workSum, wordPost[widx] + 1ull); // postings the scoring will read
-                }
+                run = lo - i;
+                widx = base + word;
+                const unsigned long long post = wordPost[widx];
+                keep = it == 0 || post < limit;
+                if (keep) myWork += post + 1ull;
             }
+            const uint32_t p = warpSlot(keep, &cnt);
+            if (keep) out[p] = Entry{level, word, run, static_cast<uint32_t>(widx)};
         }
         span *= B;
     }
+    for (uint32_t off = 16; off > 0; off >>= 1) myWork += __shfl_xor_sync(0xFFFFFFFFu, myWork, off);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(&workSum, myWork);
     __syncthreads();
     if (threadIdx.x == 0) {
         entryCount[q] = cnt;
