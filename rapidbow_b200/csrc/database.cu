@@ -543,14 +543,41 @@ __device__ __forceinline__ void selectSmallest(const unsigned long long* keys, u
                 if (key != ~0ull && (key & hiMask) == prefix) atomicAdd(&hist[(key >> shift) & 0xFFu], 1u);
             }
             __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t c = 0, d = 0;
-                for (; d < 255; d++) {
-                    if (c + hist[d] >= need) break;
-                    c += hist[d];
+            if (threadIdx.x < 32) {
+                // d = the first digit below 255 whose inclusive count reaches `need`, else 255;
+                // c = the count of the digits before d.  Lane l holds digits 8l .. 8l + 7.
+                const uint32_t lane = threadIdx.x;
+                uint32_t h[8], incl[8], run = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 8; j++) {
+                    h[j] = hist[8 * lane + j];
+                    run += h[j];
+                    incl[j] = run;
                 }
-                need -= c;
-                prefix |= static_cast<unsigned long long>(d) << shift;
+                uint32_t before = run;
+#pragma unroll
+                for (uint32_t off = 1; off < 32; off <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, before, off);
+                    if (lane >= off) before += v;
+                }
+                before -= run; // digits of the lower lanes
+                const uint32_t nd = need;
+                uint32_t jHit = 8, cHit = 0;
+#pragma unroll
+                for (int j = 7; j >= 0; j--) {
+                    if (8 * lane + j < 255 && before + incl[j] >= nd) {
+                        jHit = j;
+                        cHit = before + incl[j] - h[j];
+                    }
+                }
+                const uint32_t hitLanes = __ballot_sync(0xFFFFFFFFu, jHit < 8);
+                const uint32_t src = hitLanes ? __ffs(hitLanes) - 1 : 31u;
+                if (lane == src) {
+                    const uint32_t d = hitLanes ? 8 * lane + jHit : 255u;
+                    const uint32_t c = hitLanes ? cHit : before + incl[6]; // else digits 0 .. 254
+                    need = nd - c;
+                    prefix |= static_cast<unsigned long long>(d) << shift;
+                }
             }
             __syncthreads();
         }
