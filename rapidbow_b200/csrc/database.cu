@@ -234,9 +234,11 @@ __device__ double l1NormBlock(const uint32_t* sorted, uint32_t n, const float* w
                 int32_t e0;
                 uint32_t m;
                 split(bits, e0, m);
-                const int32_t shift = e0 - e; // >= 0: e is at most this term's lowest set bit
+                const int32_t tz = __ffs(m) - 1;
+                m >>= tz;                          // odd significand, lowest set bit 2^(e0 + tz)
+                const int32_t shift = e0 + tz - e; // >= 0: e is the lowest of those bits
                 if (shift + 32 - int32_t(__clz(m)) > 53) {
-                    bad = 1;                  // the term alone reaches 2^(e + 53)
+                    bad = 1;                       // the term alone reaches 2^(e + 53)
                     break;
                 }
                 total += static_cast<unsigned long long>(m) << shift;
