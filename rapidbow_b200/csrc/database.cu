@@ -162,11 +162,17 @@ __device__ double l1NormWarp(const uint32_t* sorted, uint32_t n, const float* we
             const float cur = next;
             const uint32_t ahead = base + 32 + lane;
             next = ahead < n ? lw[sorted[ahead] / span] : 0.f;
+            // all 32 shuffles first, so only the additions form the dependent chain
+            float t[32];
+#pragma unroll
+            for (uint32_t j = 0; j < 32; j++) t[j] = __shfl_sync(0xFFFFFFFFu, cur, j);
             if (n - base >= 32) {
 #pragma unroll
-                for (uint32_t j = 0; j < 32; j++) norm += __shfl_sync(0xFFFFFFFFu, cur, j);
+                for (uint32_t j = 0; j < 32; j++) norm += t[j];
             } else {
-                for (uint32_t j = 0; j < n - base; j++) norm += __shfl_sync(0xFFFFFFFFu, cur, j);
+#pragma unroll
+                for (uint32_t j = 0; j < 32; j++)
+                    if (j < n - base) norm += t[j];
             }
         }
         span *= B;
@@ -179,14 +185,14 @@ __device__ double l1NormWarp(const uint32_t* sorted, uint32_t n, const float* we
 // every partial sum of the reference's order is an exactly representable double, so no
 // addition in that order rounds and the in-order double sum equals the exact total, which the
 // block forms here in any order with 64-bit integers (one pass for e, one for the total).
-// Otherwise warp 0 adds the terms in order (l1NormWarp).  Call from every thread; the result
-// is valid in every thread.
-__device__ double l1NormBlock(const uint32_t* sorted, uint32_t n, const float* weights, uint32_t B, uint32_t L)
+// Call from every thread.  Returns false when some partial sum may round; the caller then adds
+// the terms in order (l1NormWarp) in one warp while the others go on.
+__device__ bool l1NormBlockExact(const uint32_t* sorted, uint32_t n, const float* weights, uint32_t B, uint32_t L,
+                                 double* norm)
 {
     __shared__ int32_t sLsb;
     __shared__ uint32_t sBad;
     __shared__ unsigned long long sTotal;
-    __shared__ double sNorm;
     if (threadIdx.x == 0) {
         sLsb = 0x7FFFFFFF;
         sBad = 0;
@@ -252,17 +258,14 @@ __device__ double l1NormBlock(const uint32_t* sorted, uint32_t n, const float* w
         if (bad) atomicOr(&sBad, 1u);
         atomicAdd(&sTotal, total);            // < blockDim * 2^53: no overflow
         __syncthreads();
-        if (!sBad && sTotal < kLimit) return ldexp(static_cast<double>(sTotal), e);
-    } else if (e == 0x7FFFFFFF && !sBad) {
-        return 0.0; // every term is zero
+        if (!sBad && sTotal < kLimit) {
+            *norm = ldexp(static_cast<double>(sTotal), e);
+            return true;
+        }
+        return false;
     }
-    // some partial sum may round: the reference's order, one term after another
-    if (threadIdx.x < 32) {
-        const double norm = l1NormWarp(sorted, n, weights, B, L);
-        if (threadIdx.x == 0) sNorm = norm;
-    }
-    __syncthreads();
-    return sNorm;
+    *norm = 0.0; // every term is zero
+    return !sBad;
 }
 
 // ------------------------------------------------------------------ documents
@@ -285,8 +288,13 @@ __global__ void __launch_bounds__(kPrepThreads) docPrepKernel(const uint32_t* ne
     uint32_t* keys = gkeys ? gkeys + uint64_t(blockIdx.x) * gstride : skeys;
     if (threadIdx.x == 0) cnt = 0;
     const uint32_t n = loadAndSort(newLeaves + (beg - docOff[s0]), nAll, keys, nbLeaves, &nValid);
-    const double norm = l1NormBlock(keys, n, weights, B, L);
-    if (threadIdx.x == 0) rcpF[slot] = float(1 / norm); // DataBase.cpp:68
+    double norm = 0;
+    if (l1NormBlockExact(keys, n, weights, B, L, &norm)) {
+        if (threadIdx.x == 0) rcpF[slot] = float(1 / norm); // DataBase.cpp:68
+    } else if (threadIdx.x < 32) {
+        norm = l1NormWarp(keys, n, weights, B, L);
+        if (threadIdx.x == 0) rcpF[slot] = float(1 / norm);
+    }
     for (uint32_t base = 0; base < n; base += blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         const uint32_t k = i < n ? keys[i] : 0u;
@@ -403,8 +411,13 @@ __global__ void __launch_bounds__(kPrepThreads) queryPrepKernel(const uint32_t* 
         workSum = 0;
     }
     const uint32_t n = loadAndSort(qLeaves + beg, nAll, keys, nbLeaves, &nValid);
-    const double norm = l1NormBlock(keys, n, weights, B, L);
-    if (threadIdx.x == 0) qRcpF[q] = float(1 / norm); // DataBase.cpp:77-94
+    double norm = 0;
+    if (l1NormBlockExact(keys, n, weights, B, L, &norm)) {
+        if (threadIdx.x == 0) qRcpF[q] = float(1 / norm); // DataBase.cpp:77-94
+    } else if (threadIdx.x < 32) {
+        norm = l1NormWarp(keys, n, weights, B, L); // while the other warps build the entries
+        if (threadIdx.x == 0) qRcpF[q] = float(1 / norm);
+    }
     uint32_t span = 1; // B^it; leaf indices are 32-bit, so is every span
     const uint64_t limit = 16ull + 4ull * k; // DataBase.h:60-61, DataBase.cpp:125
     unsigned long long myWork = 0;            // postings the scoring will read
