@@ -1044,13 +1044,13 @@ public:
         RBW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         // Document range per scoring CTA.  With grouped inverted files it is csrPerCta shards of
         // kShardDocs documents: the most (up to a group of kSmemDocs documents) that still gives
-        // two CTAs per SM, so a small batch spreads over the GPU; with one inverted file per
+        // one CTA per SM, so a small batch spreads over the GPU; with one inverted file per
         // segment, kSmemDocs documents (every CTA of a query walks the whole list).
         uint32_t csrPerCta = 1, shardDocs = std::min(std::max(nDocs, 1u), kSmemDocs);
         if (groupedIndex()) {
             csrPerCta = kSmemDocs / kShardDocs;
             while (csrPerCta > 1 &&
-                   uint64_t(nq) * ((nDocs + csrPerCta * kShardDocs - 1) / (csrPerCta * kShardDocs)) < 2ull * sms)
+                   uint64_t(nq) * ((nDocs + csrPerCta * kShardDocs - 1) / (csrPerCta * kShardDocs)) < uint64_t(sms))
                 csrPerCta /= 2;
             shardDocs = std::min(std::max(nDocs, 1u), csrPerCta * kShardDocs);
         }
