@@ -180,22 +180,34 @@ __device__ double l1NormWarp(const uint32_t* sorted, uint32_t n, const float* we
     return norm;
 }
 
-// The same sum by the whole block.  When every term is finite and >= 0, each is an integer
-// multiple of 2^e, e = the lowest set bit of any term; if the exact total is below 2^(e + 53),
-// every partial sum of the reference's order is an exactly representable double, so no
-// addition in that order rounds and the in-order double sum equals the exact total, which the
-// block forms here in any order with 64-bit integers (one pass for e, one for the total).
-// Call from every thread.  Returns false when some partial sum may round; the caller then adds
-// the terms in order (l1NormWarp) in one warp while the others go on.
+// The same sum by the whole block, when it can be shown that no addition of the reference's
+// order rounds in a way that matters.  Every term must be finite and >= 0.  Terms below 2^-70
+// ("tiny": the idf weights clamped to FLT_MIN for words in more documents than the vocabulary
+// was built for, Vocabulary.cpp:103-108) are set aside; every other term is an integer multiple
+// of 2^e, e = the lowest set bit of any of them.
+//   * If the exact total of those terms is below 2^(e + 53), each of their partial sums is an
+//     exactly representable double.
+//   * If all tiny terms together stay below 2^(m - 53), m = the exponent of the smallest other
+//     term, then every tiny term, and whatever tiny terms sum to before the first other term,
+//     is less than half an ulp of the running sum it meets (which is at least that smallest
+//     term), so it rounds away.
+// Together: the in-order double sum equals the exact total of the other terms, which the block
+// forms here in any order with 64-bit integers (one pass for the bounds, one for the total).
+// Call from every thread.  Returns false when this cannot be shown; the caller then adds the
+// terms in order (l1NormWarp) in one warp while the others go on.
 __device__ bool l1NormBlockExact(const uint32_t* sorted, uint32_t n, const float* weights, uint32_t B, uint32_t L,
                                  double* norm)
 {
+    constexpr uint32_t kTinyBits = uint32_t(127 - 70) << 23; // float bits of 2^-70
     __shared__ int32_t sLsb;
-    __shared__ uint32_t sBad;
+    __shared__ uint32_t sBad, sMinBig, sMaxTiny, sTiny;
     __shared__ unsigned long long sTotal;
     if (threadIdx.x == 0) {
         sLsb = 0x7FFFFFFF;
         sBad = 0;
+        sMinBig = 0xFFFFFFFFu;
+        sMaxTiny = 0;
+        sTiny = 0;
         sTotal = 0;
     }
     __syncthreads();
@@ -206,7 +218,7 @@ __device__ bool l1NormBlockExact(const uint32_t* sorted, uint32_t n, const float
         e0 = int32_t(ef ? ef : 1u) - 150;
     };
     int32_t lsb = 0x7FFFFFFF;
-    uint32_t bad = 0;
+    uint32_t bad = 0, minBig = 0xFFFFFFFFu, maxTiny = 0, tiny = 0;
     uint32_t span = 1;
     for (uint32_t it = 0; it < L; it++) {
         const float* lw = weights + levelBegDev(B, L - 1 - it) * B;
@@ -217,6 +229,12 @@ __device__ bool l1NormBlockExact(const uint32_t* sorted, uint32_t n, const float
                 bad = 1;                              // negative, infinite or NaN
                 continue;
             }
+            if (bits < kTinyBits) {                   // positive floats order like their bits
+                tiny++;
+                maxTiny = max(maxTiny, bits);
+                continue;
+            }
+            minBig = min(minBig, bits);
             int32_t e0;
             uint32_t m;
             split(bits, e0, m);
@@ -226,46 +244,59 @@ __device__ bool l1NormBlockExact(const uint32_t* sorted, uint32_t n, const float
     }
     atomicMin(&sLsb, lsb);
     if (bad) atomicOr(&sBad, 1u);
+    if (tiny) {
+        atomicAdd(&sTiny, tiny);
+        atomicMax(&sMaxTiny, maxTiny);
+    }
+    atomicMin(&sMinBig, minBig);
     __syncthreads();
     const int32_t e = sLsb;
-    if (!sBad && e != 0x7FFFFFFF) {
-        constexpr unsigned long long kLimit = 1ull << 53;
-        unsigned long long total = 0;
-        span = 1;
-        for (uint32_t it = 0; it < L && !bad; it++) {
-            const float* lw = weights + levelBegDev(B, L - 1 - it) * B;
-            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-                const uint32_t bits = __float_as_uint(lw[sorted[i] / span]);
-                if ((bits & 0x7FFFFFFFu) == 0) continue;
-                int32_t e0;
-                uint32_t m;
-                split(bits, e0, m);
-                const int32_t tz = __ffs(m) - 1;
-                m >>= tz;                          // odd significand, lowest set bit 2^(e0 + tz)
-                const int32_t shift = e0 + tz - e; // >= 0: e is the lowest of those bits
-                if (shift + 32 - int32_t(__clz(m)) > 53) {
-                    bad = 1;                       // the term alone reaches 2^(e + 53)
-                    break;
-                }
-                total += static_cast<unsigned long long>(m) << shift;
-                if (total >= kLimit) {
-                    bad = 1;
-                    break;
-                }
-            }
-            span *= B;
-        }
-        if (bad) atomicOr(&sBad, 1u);
-        atomicAdd(&sTotal, total);            // < blockDim * 2^53: no overflow
-        __syncthreads();
-        if (!sBad && sTotal < kLimit) {
-            *norm = ldexp(static_cast<double>(sTotal), e);
-            return true;
-        }
-        return false;
+    bool ok = !sBad;
+    if (ok && sTiny) {
+        // all tiny terms < sTiny * 2^(exp(maxTiny) + 1) <= 2^(ceil(log2 sTiny) + exp(maxTiny) + 1);
+        // one more factor of two covers the rounding of their own in-order sum
+        const int32_t expTiny = int32_t((sMaxTiny >> 23) & 0xFFu) - 127;
+        const int32_t logCount = 32 - int32_t(__clz(sTiny - 1u)); // ceil(log2(sTiny)), 0 for 1
+        const int32_t expBig = int32_t((sMinBig >> 23) & 0xFFu) - 127;
+        ok = sMinBig != 0xFFFFFFFFu && logCount + expTiny + 2 <= expBig - 53;
     }
-    *norm = 0.0; // every term is zero
-    return !sBad;
+    if (!ok) return false;
+    if (e == 0x7FFFFFFF) {
+        *norm = 0.0; // no term above the tiny ones (and none of those)
+        return sTiny == 0;
+    }
+    constexpr unsigned long long kLimit = 1ull << 53;
+    unsigned long long total = 0;
+    span = 1;
+    for (uint32_t it = 0; it < L && !bad; it++) {
+        const float* lw = weights + levelBegDev(B, L - 1 - it) * B;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t bits = __float_as_uint(lw[sorted[i] / span]);
+            if ((bits & 0x7FFFFFFFu) == 0 || bits < kTinyBits) continue;
+            int32_t e0;
+            uint32_t m;
+            split(bits, e0, m);
+            const int32_t tz = __ffs(m) - 1;
+            m >>= tz;                          // odd significand, lowest set bit 2^(e0 + tz)
+            const int32_t shift = e0 + tz - e; // >= 0: e is the lowest of those bits
+            if (shift + 32 - int32_t(__clz(m)) > 53) {
+                bad = 1;                       // the term alone reaches 2^(e + 53)
+                break;
+            }
+            total += static_cast<unsigned long long>(m) << shift;
+            if (total >= kLimit) {
+                bad = 1;
+                break;
+            }
+        }
+        span *= B;
+    }
+    if (bad) atomicOr(&sBad, 1u);
+    atomicAdd(&sTotal, total); // < blockDim * 2^53: no overflow
+    __syncthreads();
+    if (sBad || sTotal >= kLimit) return false;
+    *norm = ldexp(static_cast<double>(sTotal), e);
+    return true;
 }
 
 // ------------------------------------------------------------------ documents

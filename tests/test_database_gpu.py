@@ -108,6 +108,39 @@ def test_postings_norms_and_queries(oracle, B, L, n_docs):
             check_query(db, odb, q, k)
 
 
+@pytest.mark.parametrize("kind", ["idf_clamped", "wide_spread", "tiny_only_upper"])
+def test_norms_bit_exact_for_every_weight_spread(oracle, kind):
+    """Document and query norms are the reference's in-order double sums for every spread of
+    weights: idf weights with the FLT_MIN clamp of common words (the block's exact sum sets the
+    tiny terms aside), weights 2^-30 apart among the others (the in-order fallback), and words
+    whose every upper level is clamped."""
+    B, L = 10, 3
+    rng = np.random.default_rng(61)
+    centers, masks, weights = random_tree(B, L, 62, dup_rate=0.0)
+    fmin = np.float32(np.finfo(np.float32).tiny)
+    if kind == "idf_clamped":
+        weights = np.log(rng.uniform(1.0, 5e4, weights.shape)).astype(np.float32)
+        weights[:1 + B] = fmin                       # levels 0 and 1: in every document
+        weights[rng.random(weights.shape) < 0.05] = fmin
+    elif kind == "wide_spread":
+        weights = rng.uniform(0.5, 12.0, weights.shape).astype(np.float32)
+        weights[rng.random(weights.shape) < 0.3] = np.float32(3e-9)
+    else:
+        weights[:1 + B] = fmin
+        weights[rng.random(weights.shape) < 0.5] = fmin
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    db = rbw.DataBase(voc)
+    odb = oracle.db(B, L, weights)
+    docs = make_docs(300, B ** L, seed=63, lo=1, hi=3000)
+    for i, d in enumerate(docs):
+        db.add_doc(i, d)
+        odb.add(i, d)
+    for i in range(len(docs)):
+        assert np.float32(db.doc_rcp(i)) == np.float32(odb.doc_rcp(i)), i
+    for q in make_queries(docs, B ** L, 12, seed=64):
+        check_query(db, odb, q, 25)
+
+
 def test_self_query_ranks_itself_first(oracle):
     B, L = 16, 3
     docs = make_docs(200, B ** L, seed=3)
