@@ -665,6 +665,7 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
 {
     extern __shared__ unsigned long long dyn[];
     __shared__ uint32_t nTouched;
+    __shared__ uint32_t nextBatch; // entry batches are handed to warps as they finish
     __shared__ unsigned long long sel[kMaxK];
     const uint32_t q = P.order ? P.order[blockIdx.x] : blockIdx.x;
     const uint32_t shard = blockIdx.y;
@@ -679,10 +680,13 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
         acc[i] = 0;
         touched[i] = 0;
     }
-    if (threadIdx.x == 0) nTouched = 0;
+    if (threadIdx.x == 0) {
+        nTouched = 0;
+        nextBatch = 0;
+    }
     __syncthreads();
 
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nWarpsCta = blockDim.x >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
     const Entry* ent = P.entries + (P.qOff[q] - P.qOff[0]) * P.L;
     const uint32_t ne = P.entryCount[q];
     const float qRcp = P.qRcpF[q];
@@ -749,7 +753,11 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
     // Leaf lists shorter than kFlatList are then walked as one range over the batch (lane t of
     // a round takes pair t of the concatenated lists, kFlatDepth pairs per lane in flight);
     // longer lists and non-leaf words go one at a time with the whole warp.
-    for (uint32_t base = warp * 32u; base < ne; base += nWarpsCta * 32u) {
+    for (;;) {
+        uint32_t batch = 0;
+        if (lane == 0) batch = atomicAdd(&nextBatch, 1u);
+        const uint32_t base = __shfl_sync(0xFFFFFFFFu, batch, 0) * 32u;
+        if (base >= ne) break;
         const uint32_t e = base + lane;
         const bool valid = e < ne;
         float qv = 0.f, w = 0.f;
