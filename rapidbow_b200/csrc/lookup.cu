@@ -1168,16 +1168,76 @@ __global__ void __launch_bounds__(1024) regroupScan(uint32_t* ctaHist, uint32_t 
     }
 }
 
+// Chunks of kScatterChunk rows are grouped by bin in shared memory first, so each bin's rows of a
+// chunk leave as one contiguous run of the permutation (whole sectors) rather than as scattered
+// 4-byte stores.
+constexpr uint32_t kScatterChunk = 8192;
+constexpr uint32_t kScatterPerThread = kScatterChunk / kRegroupThreads;
+constexpr size_t kScatterSmemBytes = size_t(kScatterChunk) * 6 + 2 * kSmemHistMax * 4;
+
 __global__ void __launch_bounds__(kRegroupThreads) regroupScatter(const uint32_t* nodeNext, uint64_t n, uint64_t per,
                                                                   uint32_t nb, const uint32_t* ctaOff, uint32_t* perm)
 {
-    __shared__ uint32_t next[kSmemHistMax];
+    extern __shared__ uint32_t smemScatter[];
+    uint32_t* next = smemScatter;                  // [nb] position of this CTA's next row per bin
+    uint32_t* cnt = next + kSmemHistMax;           // [nb] rows of the chunk per bin, then offsets
+    uint32_t* stage = cnt + kSmemHistMax;          // [kScatterChunk] row ids grouped by bin
+    uint16_t* stageBin = reinterpret_cast<uint16_t*>(stage + kScatterChunk);
     for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) next[i] = ctaOff[uint64_t(blockIdx.x) * nb + i];
-    __syncthreads();
     uint64_t beg, end;
     regroupRange(n, per, beg, end);
-    forEachRow(nodeNext, beg, end,
-               [&](uint32_t node, uint64_t r) { perm[atomicAdd(&next[node], 1u)] = static_cast<uint32_t>(r); });
+    for (uint64_t c0 = beg; c0 < end; c0 += kScatterChunk) {
+        const uint32_t rows = static_cast<uint32_t>(end - c0 < kScatterChunk ? end - c0 : kScatterChunk);
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) cnt[i] = 0;
+        __syncthreads();
+        uint32_t node[kScatterPerThread], rank[kScatterPerThread];
+#pragma unroll
+        for (uint32_t k = 0; k < kScatterPerThread; k++) {
+            const uint32_t j = k * kRegroupThreads + threadIdx.x;
+            node[k] = j < rows ? __ldg(nodeNext + c0 + j) : 0u;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kScatterPerThread; k++)
+            if (k * kRegroupThreads + threadIdx.x < rows) rank[k] = atomicAdd(&cnt[node[k]], 1u);
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            // exclusive scan of the chunk's bin counts in place (lane l: bins 32 l .. 32 l + 31)
+            const uint32_t lane = threadIdx.x;
+            uint32_t sum = 0;
+            for (uint32_t i = 32 * lane; i < 32 * lane + 32 && i < nb; i++) sum += cnt[i];
+            uint32_t incl = sum;
+#pragma unroll
+            for (uint32_t off = 1; off < 32; off <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+                if (lane >= off) incl += v;
+            }
+            uint32_t run = incl - sum;
+            for (uint32_t i = 32 * lane; i < 32 * lane + 32 && i < nb; i++) {
+                const uint32_t c = cnt[i];
+                cnt[i] = run;
+                run += c;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t k = 0; k < kScatterPerThread; k++) {
+            const uint32_t j = k * kRegroupThreads + threadIdx.x;
+            if (j < rows) {
+                const uint32_t at = cnt[node[k]] + rank[k];
+                stage[at] = static_cast<uint32_t>(c0 + j);
+                stageBin[at] = static_cast<uint16_t>(node[k]);
+            }
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < rows; j += blockDim.x) {
+            const uint32_t bn = stageBin[j];
+            perm[next[bn] + (j - cnt[bn])] = stage[j];
+        }
+        __syncthreads();
+        // the chunk's count of bin b is the distance to the next bin's offset
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) next[i] += (i + 1 < nb ? cnt[i + 1] : rows) - cnt[i];
+        __syncthreads();
+    }
 }
 
 // ------------------------------------------------------------------ plain FP32 SIMT kernel
@@ -1363,7 +1423,9 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
     }
     const bool warpNode = algo == kLookupTensorU8WarpNode;
     const bool ring = algo == kLookupTensorU8Ring;
-    static std::atomic<uint64_t> attrSet{0}, attrSetW{0}, attrSetR{0};
+    static std::atomic<uint64_t> attrSet{0}, attrSetW{0}, attrSetR{0}, attrSetS{0};
+    setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(regroupScatter), static_cast<int>(kScatterSmemBytes),
+                                   attrSetS);
     if (ring) {
         setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(lookupPassRing),
                                        static_cast<int>(kTcSmemBytes), attrSetR);
@@ -1439,8 +1501,8 @@ uint32_t launchLookup(const DeviceTree& tree, const uint8_t* desc, uint64_t n, u
                 regroupScan<<<1, 1024, 0, stream>>>(scratch.ctaHist, kRegroupCtas, nbBins, count, rowOff, tileOff,
                                                     totals);
                 buildTiles<<<tileBlocks, 256, 0, stream>>>(count, rowOff, tileOff, nbBins, totals, maxTiles, tiles);
-                regroupScatter<<<kRegroupCtas, kRegroupThreads, 0, stream>>>(scratch.nodeNext, n, per, nbBins,
-                                                                            scratch.ctaHist, scratch.perm);
+                regroupScatter<<<kRegroupCtas, kRegroupThreads, kScatterSmemBytes, stream>>>(
+                    scratch.nodeNext, n, per, nbBins, scratch.ctaHist, scratch.perm);
                 RBW_CUDA(cudaGetLastError());
                 kernels += 4;
                 continue;
