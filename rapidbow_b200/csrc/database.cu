@@ -1161,17 +1161,10 @@ public:
             P.outDocs = dDocs;
             P.outScores = dScores;
             P.outCount = dCount;
+            // 1,024 threads per CTA whatever its document range: the pair walk is bound by load
+            // latency, so a query split over few CTAs needs every warp an SM can hold
             const size_t smem = size_t(shardDocs) * 9;
-            // threads per CTA with its documents: 256 up to 2,560, 512 up to 10,240, else 1024
-            const uint32_t threads = shardDocs <= kShardDocs ? 256u : shardDocs <= 4 * kShardDocs ? 512u : 1024u;
-            const dim3 grid(nq, shards);
-            if (threads == 256) {
-                launchScore<256>(shards > 1, grid, smem, stream, P);
-            } else if (threads == 512) {
-                launchScore<512>(shards > 1, grid, smem, stream, P);
-            } else {
-                launchScore<1024>(shards > 1, grid, smem, stream, P);
-            }
+            launchScore<kScoreThreads>(shards > 1, dim3(nq, shards), smem, stream, P);
             if (shards > 1) {
                 ScopedKernelTimer mergeTimer(kTimedScoreMerge, stream);
                 mergeKernel<<<nq, kScoreThreads, 0, stream>>>(P, shards);
