@@ -701,9 +701,22 @@ def serving_bench(args, dev, rank):
     qpool = sift_like(4_000_000, seed=4, n_components=4096, zipf=1.1, device=dev).cpu().numpy()
     torch.cuda.empty_cache()
     srv = rbw.Server(voc, db, max_results=100)
-    # warm-up (also builds the index)
+    # warm-up (also builds the index): a few requests alone, then 0.25 s of the same Poisson
+    # stream, so that buffers of every size the run will use exist before the timed region
     for _ in range(3):
         srv.wait(srv.submit(qpool[:2000]))
+    warm_n = int(args.serving_rate * 0.25)
+    warm_gaps = rng.exponential(1.0 / args.serving_rate, warm_n)
+    warm_sizes = np.exp(rng.uniform(np.log(300), np.log(8000), warm_n)).astype(np.int64)
+    warm_ids = []
+    t_next = time.perf_counter()
+    for i in range(warm_n):
+        t_next += warm_gaps[i]
+        while time.perf_counter() < t_next:
+            pass
+        warm_ids.append(srv.submit(qpool[i * 97 % (qpool.shape[0] - 8000):][: warm_sizes[i]]))
+    for i in warm_ids:
+        srv.wait(i)
     srv.reset_stats()
 
     n_req = int(args.serving_rate * args.serving_seconds)

@@ -149,6 +149,23 @@ public:
             while (hi < 20 && (size_t(1) << hi) < mOpt.max_batch_descriptors * 128) hi++;
             mPinned.reserve(16, hi, 8);
         }
+        {
+            // Grow the device pool once, to what every slot needs for a batch of up to 65,536
+            // descriptors: the pool keeps freed memory, so batches of that size never wait for the
+            // pool to grow (a growth is a driver call that holds up the dispatcher).
+            const uint64_t warmDesc = std::min<uint64_t>(mOpt.max_batch_descriptors, 65536);
+            const uint64_t warmQueries = std::min<uint64_t>(mOpt.max_batch_queries, 64);
+            const size_t bytes = std::min<size_t>(2 * estimate(warmDesc, warmQueries) * mSlots.size(),
+                                                  mOpt.hbm_budget_bytes);
+            void* p = nullptr;
+            cudaStream_t s0 = mSlots[0].stream;
+            if (cudaMallocFromPoolAsync(&p, bytes, libraryPool(), s0) == cudaSuccess) {
+                RBW_CUDA(cudaFreeAsync(p, s0));
+            } else {
+                cudaGetLastError(); // a smaller pool only means growth later
+            }
+            RBW_CUDA(cudaStreamSynchronize(s0));
+        }
         mDispatcher = std::thread([this] { dispatchLoop(); });
         mCompleter = std::thread([this] { completeLoop(); });
     }
