@@ -760,6 +760,8 @@ def serving_bench(args, dev, rank):
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
             "mean_batch_requests": st["mean_batch_requests"], "batches": st["batches"],
             "max_inflight_batches_seen": st["max_inflight_seen"], "descriptors_per_request_mean": float(qs.mean()),
+            "latency_stages_ms": {k: st[k] for k in ("queue_p99_ms", "launch_p99_ms", "device_p99_ms", "queue_max_ms",
+                                                      "launch_max_ms", "device_max_ms")},
             "db_postings": int(sizes.sum()), "gpu_event_ms_by_kernel": kernels,
             "note": "latency = submit to result on the host, including the host-to-device copy of the descriptors; "
                     "kernel times are event spans on streams that share the GPU"}

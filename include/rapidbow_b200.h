@@ -295,6 +295,11 @@ typedef struct {
     uint32_t max_inflight_seen;     /* most batches on the GPU at once */
     double mean_batch_requests;
     double p50_ms, p99_ms, max_ms;  /* latency from submit to result, completed requests */
+    /* the same latency in three stages, p99 and max of each: waiting for a batch (submit to
+     * dispatch), the host's launch of the batch, and the batch on the device until its result
+     * is collected */
+    double queue_p99_ms, launch_p99_ms, device_p99_ms;
+    double queue_max_ms, launch_max_ms, device_max_ms;
 } rbw_server_stats;
 
 RBW_API void rbw_server_options_default(rbw_server_options* opts);

@@ -93,7 +93,7 @@ struct Request {
     uint8_t* desc = nullptr;     // pinned, n x 128 (from the server's pool)
     uint32_t descClass = 0;
     uint32_t n = 0;
-    Clock::time_point submitted, finished;
+    Clock::time_point submitted, dispatched, launched, finished;
     bool done = false;
     int status = 0;
     std::string error;
@@ -247,15 +247,21 @@ public:
         st->max_inflight_seen = mMaxInflight;
         st->mean_batch_requests = mBatches ? double(mBatchedRequests) / double(mBatches) : 0.0;
         if (!mLatencies.empty()) {
-            std::vector<double> l = mLatencies;
-            auto pct = [&](double p) {
+            auto pct = [](std::vector<double> l, double p) {
                 const size_t i = std::min(l.size() - 1, static_cast<size_t>(p * double(l.size() - 1) + 0.5));
                 std::nth_element(l.begin(), l.begin() + i, l.end());
                 return l[i];
             };
-            st->p50_ms = pct(0.50);
-            st->p99_ms = pct(0.99);
-            st->max_ms = *std::max_element(l.begin(), l.end());
+            auto maxOf = [](const std::vector<double>& l) { return *std::max_element(l.begin(), l.end()); };
+            st->p50_ms = pct(mLatencies, 0.50);
+            st->p99_ms = pct(mLatencies, 0.99);
+            st->max_ms = maxOf(mLatencies);
+            st->queue_p99_ms = pct(mStage[0], 0.99);
+            st->launch_p99_ms = pct(mStage[1], 0.99);
+            st->device_p99_ms = pct(mStage[2], 0.99);
+            st->queue_max_ms = maxOf(mStage[0]);
+            st->launch_max_ms = maxOf(mStage[1]);
+            st->device_max_ms = maxOf(mStage[2]);
         }
     }
 
@@ -265,6 +271,7 @@ public:
     {
         std::lock_guard<std::mutex> lk(mMu);
         mLatencies.clear();
+        for (auto& v : mStage) v.clear();
         mBatches = mBatchedRequests = 0;
         mMaxInflight = 0;
         mSubmitted = 0;
@@ -354,6 +361,8 @@ private:
                 slot->reqs.push_back(r);
                 mPending.pop_front();
             }
+            const Clock::time_point formed = Clock::now();
+            for (auto& r : slot->reqs) r->dispatched = formed;
             slot->reserved = estimate(desc, slot->reqs.size());
             mReserved += slot->reserved;
             mLiveFree = mLiveFree > slot->reserved ? mLiveFree - slot->reserved : 0;
@@ -365,7 +374,9 @@ private:
             mMaxInflight = std::max(mMaxInflight, inflight);
             lk.unlock();
             launch(*slot, desc);
+            const Clock::time_point launched = Clock::now();
             lk.lock();
+            for (auto& r : slot->reqs) r->launched = launched;
             mInflight.push_back(slot);
             mCv.notify_all();
         }
@@ -476,8 +487,15 @@ private:
         // the batch that copied these descriptors has completed (or never ran)
         mPinned.give(r.desc, r.descClass);
         r.desc = nullptr;
-        if (status == RBW_OK)
-            mLatencies.push_back(std::chrono::duration<double, std::milli>(r.finished - r.submitted).count());
+        if (status == RBW_OK) {
+            auto ms = [](Clock::time_point a, Clock::time_point b) {
+                return std::chrono::duration<double, std::milli>(b - a).count();
+            };
+            mLatencies.push_back(ms(r.submitted, r.finished));
+            mStage[0].push_back(ms(r.submitted, r.dispatched));
+            mStage[1].push_back(ms(r.dispatched, r.launched));
+            mStage[2].push_back(ms(r.launched, r.finished));
+        }
     }
 
     PinnedPool mPinned; // destroyed after the threads (declared before them)
@@ -493,6 +511,7 @@ private:
     std::deque<Slot*> mInflight;
     std::unordered_map<uint64_t, std::shared_ptr<Request>> mAll;
     std::vector<double> mLatencies;
+    std::vector<double> mStage[3]; // queue, launch, device (ms), as mLatencies
     uint64_t mNextId = 0, mSubmitted = 0, mBatches = 0, mBatchedRequests = 0;
     uint32_t mMaxInflight = 0;
     size_t mReserved = 0;

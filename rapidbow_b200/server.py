@@ -19,7 +19,9 @@ class ServerOptions(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
                 ("max_inflight_seen", C.c_uint32), ("mean_batch_requests", C.c_double),
-                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double)]
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+                ("queue_p99_ms", C.c_double), ("launch_p99_ms", C.c_double), ("device_p99_ms", C.c_double),
+                ("queue_max_ms", C.c_double), ("launch_max_ms", C.c_double), ("device_max_ms", C.c_double)]
 
 
 class Server:
