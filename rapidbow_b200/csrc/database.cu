@@ -919,16 +919,22 @@ struct Segment {
     }
 };
 
+// The kernels' dynamic shared-memory limits are raised once per device to the largest size any
+// launch uses: changing a function's attribute between launches can wait for that function's
+// launches in flight on other streams.
+constexpr int kPrepSmemMax = int(kMaxDocDesc) * 4;
+constexpr int kScoreSmemMax = int(kSmemDocs) * 9;
+
 template <uint32_t kThreads>
 void launchScore(bool sharded, dim3 grid, size_t smem, cudaStream_t stream, const ScoreParams& P)
 {
+    static std::atomic<uint64_t> setS{0}, setU{0};
     if (sharded) {
-        RBW_CUDA(cudaFuncSetAttribute(scoreKernel<true, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(smem)));
+        setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(scoreKernel<true, kThreads>), kScoreSmemMax, setS);
         scoreKernel<true, kThreads><<<grid, kThreads, smem, stream>>>(P);
     } else {
-        RBW_CUDA(cudaFuncSetAttribute(scoreKernel<false, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(smem)));
+        setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(scoreKernel<false, kThreads>), kScoreSmemMax,
+                                       setU);
         scoreKernel<false, kThreads><<<grid, kThreads, smem, stream>>>(P);
     }
     RBW_CUDA(cudaGetLastError());
@@ -1115,7 +1121,8 @@ public:
             ScopedKernelTimer timer(kTimedScore, stream);
             std::optional<ScopedKernelTimer> prepTimer(std::in_place, kTimedScorePrep, stream);
             const size_t prepSmem = size_t(nextPow2(std::max(maxN, 1u))) * 4;
-            RBW_CUDA(cudaFuncSetAttribute(queryPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(prepSmem)));
+            static std::atomic<uint64_t> setPrep{0};
+            setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(queryPrepKernel), kPrepSmemMax, setPrep);
             queryPrepKernel<<<nq, kPrepThreads, prepSmem, stream>>>(
                 dLeaves, dOff, nullptr, nullptr, 0u, mWeights.as<float>(), skipCounts(), mB, mL,
                 mNbLeaves, k, static_cast<float*>(qr), static_cast<Entry*>(ent), static_cast<uint32_t*>(cnt), work);
@@ -1408,7 +1415,8 @@ private:
         if (p1 > p0)
             RBW_CUDA(cudaMemcpyAsync(newLeaves, mStage.data(), (p1 - p0) * 4, cudaMemcpyHostToDevice, mStream));
         const size_t smem = size_t(nextPow2(std::max(mStageMaxN, 1u))) * 4;
-        RBW_CUDA(cudaFuncSetAttribute(docPrepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        static std::atomic<uint64_t> setDoc{0};
+        setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(docPrepKernel), kPrepSmemMax, setDoc);
         docPrepKernel<<<s1 - s0, kPrepThreads, smem, mStream>>>(
             static_cast<const uint32_t*>(newLeaves), mDocOff.as<uint64_t>(), s0, nullptr, nullptr, 0u,
             mWeights.as<float>(), mB, mL, mNbLeaves, mRcpF.as<float>(), mDocPairs.as<uint64_t>(),
