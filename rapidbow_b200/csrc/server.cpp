@@ -144,10 +144,12 @@ public:
             RBW_CUDA(cudaMallocHost(&s.hCount, q * 4));
         }
         {
-            // requests of up to 8,192 descriptors find a pinned buffer ready
+            // Requests of up to 8,192 descriptors find a pinned buffer ready, 32 per size class
+            // (waiting and in-flight requests together): a page-locked allocation during serving
+            // is a driver call that can hold up the other threads' CUDA calls for milliseconds.
             uint32_t hi = 16;
             while (hi < 20 && (size_t(1) << hi) < mOpt.max_batch_descriptors * 128) hi++;
-            mPinned.reserve(16, hi, 8);
+            mPinned.reserve(16, hi, 32);
         }
         {
             // Grow the device pool once, to what every slot needs for a batch of up to 65,536
