@@ -547,7 +547,9 @@ __device__ __forceinline__ float termOf(float q, float d) { return fabsf(q - d) 
 // Adds a term to a document of this CTA's shard (local index `i` < shard size).
 __device__ __forceinline__ void addTerm(unsigned long long* acc, uint8_t* touched, uint32_t i, float term)
 {
-    const long long fx = llrint(static_cast<double>(term) * kFixScale);
+    // term * 2^56 is exact in fp32 (|term| <= 2, a power-of-two scale), so rounding it to the
+    // nearest integer in fp32 gives the value llrint(double(term) * 2^56) would, without FP64
+    const long long fx = __float2ll_rn(term * 0x1p56f);
     atomicAdd(&acc[i], static_cast<unsigned long long>(fx));
     touched[i] = 1; // every writer stores the same value
 }
