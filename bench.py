@@ -271,14 +271,15 @@ def run_ours(args, world, rank, local):
             timed.regroup = rbw.timing_read("lookup_regroup")
         return allreduce_max(world, ms), launches, kern
 
-    # autotuning (before the timed region): rows per thread of the regroup scatter, on this lookup
+    # autotuning (before the timed region): the tensor-core schedule of algo "auto", on this lookup
     tuned = None
     if not args.no_tune:
         from rapidbow_b200.autotune import Autotuner
 
         e = Autotuner.for_current_device().tune_lookup(voc, desc)
-        tuned = {"param": "scatter_rows", "value": e["value"], "default": 16, "tuned_ms": e["ms"],
-                 "default_ms": e["default_ms"], "kernel": "scanBins + buildTiles + scatterRows (per lookup)"}
+        tuned = {"param": "lookup_schedule", "value": e["value"], "default": 1, "tuned_ms": e["ms"],
+                 "default_ms": e["default_ms"], "candidates_ms": e["candidates"],
+                 "kernel": "tensor-core pass (1 = level pairs in two buffers, 2 = three-slot ring), per launch"}
     with ClockSampler(local) as clocks:
         ms, launches, (k_ms, k_n) = timed(args.algo, args.steps, args.warmup, "lookup_pass_tc")
     regroup_ms, regroup_n = timed.regroup
@@ -290,6 +291,8 @@ def run_ours(args, world, rank, local):
 
     value = world * n / (ms / 1e3)
     fp32_value = world * n / (ms_simt / 1e3)
+    ring = args.algo == "tensor_u8_ring" or (args.algo == "auto" and tuned is not None and tuned["value"] == 2)
+    pass_kernel = "lookupPassRing" if ring else "lookupPassTc"
     hbm_peak, peak_kind = peaks()
     k_avg_ms = k_ms / max(k_n, 1)
     achieved = n * BYTES_PER_DESC / (k_avg_ms / 1e3) / 1e9
@@ -309,7 +312,7 @@ def run_ours(args, world, rank, local):
                       "speedup": value / fp32_value, "kernel": "lookupSimtF32"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "lookupPassTc", "launch_ms": k_avg_ms, "launches_per_step": k_n / args.steps,
+                     "kernel": pass_kernel, "launch_ms": k_avg_ms, "launches_per_step": k_n / args.steps,
                      "algorithmic_bytes_per_launch": n * BYTES_PER_DESC},
         "whole_lookup_hbm_frac": (n * BYTES_PER_DESC / (ms / 1e3) / 1e9) / hbm_peak,
         "regroup": {"ms_per_step": regroup_ms / args.steps, "regroups_per_step": regroup_n / args.steps,

@@ -376,9 +376,11 @@ enum {
     RBW_TUNE_ASSIGN_CTAS_PER_SM = 0,     /* uint8 k-means assign: CTAs per SM, 1..6 (default 6) */
     RBW_TUNE_ASSIGN_F32_CTAS_PER_SM = 1, /* float-center assign: CTAs per SM, 1..3 (default 3) */
     RBW_TUNE_SCATTER_ROWS = 2,           /* lookup regroup: rows per thread, 8, 16 or 32 (default 16) */
-    RBW_TUNE_DB_SHARD_TABLES = 3         /* DataBase inverted file, keyed by documents instead of
-                                            descriptors: 1 one CSR per 2,560-document shard while
-                                            those tables stay small (default), 2 one CSR */
+    RBW_TUNE_DB_SHARD_TABLES = 3,        /* DataBase inverted file, keyed by documents instead of
+                                            descriptors: 1 grouped tables per 2,560-document shard
+                                            while those tables stay small (default), 2 one CSR */
+    RBW_TUNE_LOOKUP_SCHEDULE = 4         /* the tensor-core schedule RBW_LOOKUP_AUTO runs: 1 level
+                                            pairs in two buffers (default), 2 the three-slot ring */
 };
 /* value 0 removes the entry; RBW_ERR_INVALID_ARG for a value the parameter cannot take. */
 RBW_API int rbw_tuning_set(uint32_t param, uint32_t branch_factor, uint32_t nb_levels, uint32_t bucket,

@@ -7,7 +7,10 @@ tree levels, descriptor-count bucket = floor(log2(n))):
 
     assign_ctas_per_sm      uint8 k-means assign, CTAs per SM: 2..6         (default 6)
     assign_f32_ctas_per_sm  float-center assign, CTAs per SM: 1..3          (default 3)
-    scatter_rows            lookup regroup scatter, rows per thread: 8|16|32 (default 16)
+    scatter_rows            lookup regroup scatter of more than 1,024 bins, rows per thread:
+                            8|16|32 (default 16)
+    lookup_schedule         tensor-core lookup schedule of algo "auto": 1 level pairs in two
+                            accumulator buffers, 2 the three-slot ring (default 1)
     db_shard_tables         DataBase inverted file: 1 one CSR per 2,560-document shard while
                             small, 2 one CSR (default 1; its bucket counts documents)
 
@@ -29,10 +32,12 @@ import numpy as np
 
 from . import _check, load_library
 
-PARAMS = {"assign_ctas_per_sm": 0, "assign_f32_ctas_per_sm": 1, "scatter_rows": 2, "db_shard_tables": 3}
-DEFAULTS = {"assign_ctas_per_sm": 6, "assign_f32_ctas_per_sm": 3, "scatter_rows": 16, "db_shard_tables": 1}
+PARAMS = {"assign_ctas_per_sm": 0, "assign_f32_ctas_per_sm": 1, "scatter_rows": 2, "db_shard_tables": 3,
+          "lookup_schedule": 4}
+DEFAULTS = {"assign_ctas_per_sm": 6, "assign_f32_ctas_per_sm": 3, "scatter_rows": 16, "db_shard_tables": 1,
+            "lookup_schedule": 1}
 CANDIDATES = {"assign_ctas_per_sm": (2, 3, 4, 5, 6), "assign_f32_ctas_per_sm": (1, 2, 3), "scatter_rows": (8, 16, 32),
-              "db_shard_tables": (1, 2)}
+              "db_shard_tables": (1, 2), "lookup_schedule": (1, 2)}
 FORMAT = "rapidbow_b200 tuning cache"
 VERSION = 1
 
@@ -167,8 +172,30 @@ class Autotuner:
         return self.tune(param, B, 0, n, measure)
 
     def tune_lookup(self, voc, desc, repeats: int = 3) -> dict:
-        """Tunes the regroup scatter on lookups of `desc` through `voc`, timed by the library's
-        regroup events."""
+        """Tunes the tensor-core schedule of algo "auto" on lookups of `desc` through `voc`, timed
+        by the library's pass events."""
+        import torch
+
+        from . import timing_enable, timing_read, timing_reset
+
+        out = torch.empty(desc.shape[0], dtype=torch.int32, device=desc.device)
+
+        def measure() -> float:
+            voc.lookup(desc, out)
+            torch.cuda.synchronize()
+            timing_reset()
+            timing_enable(True)
+            for _ in range(repeats):
+                voc.lookup(desc, out)
+            torch.cuda.synchronize()
+            timing_enable(False)
+            return timing_read("lookup_pass_tc")[0] / repeats
+
+        return self.tune("lookup_schedule", voc.branch_factor, voc.nb_levels, desc.shape[0], measure)
+
+    def tune_lookup_regroup(self, voc, desc, repeats: int = 3) -> dict:
+        """Tunes the scatter of regroups of more than 1,024 bins (trees with B^(2p+2) > 1,024 at a
+        pass boundary) on lookups of `desc`, timed by the library's regroup events."""
         import torch
 
         from . import timing_enable, timing_read, timing_reset

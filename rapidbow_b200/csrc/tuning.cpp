@@ -19,6 +19,7 @@ bool valid(TuneParam p, uint32_t v)
     case kTuneAssignFCtasPerSm: return v >= 1 && v <= 3;
     case kTuneScatterRows: return v == 8 || v == 16 || v == 32;
     case kTuneDbShardTables: return v == 1 || v == 2;
+    case kTuneLookupSchedule: return v == 1 || v == 2;
     default: return false;
     }
 }
@@ -42,6 +43,7 @@ uint32_t tuneDefault(TuneParam p)
     case kTuneAssignFCtasPerSm: return 3;
     case kTuneScatterRows: return 16;
     case kTuneDbShardTables: return 1;
+    case kTuneLookupSchedule: return 1;
     default: return 0;
     }
 }

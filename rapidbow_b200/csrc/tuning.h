@@ -11,7 +11,8 @@ enum TuneParam : uint32_t {
     kTuneAssignFCtasPerSm = 1, // float-center assign: resident CTAs per SM, 1..3 (default 3)
     kTuneScatterRows = 2,      // lookup regroup scatter: rows per thread, 8 | 16 | 32 (default 16)
     kTuneDbShardTables = 3,    // inverted file: 1 one CSR per 2,560-document shard while small (default), 2 one CSR
-    kTuneParamCount = 4,
+    kTuneLookupSchedule = 4,   // tensor-core lookup of RBW_LOOKUP_AUTO: 1 pair schedule (default), 2 ring
+    kTuneParamCount = 5,
 };
 
 // floor(log2(max(n, 1))): workloads within a factor of two share an entry.

@@ -5,6 +5,7 @@
 //   deserialize  : Vocabulary.cpp:126-157
 #include "vocabulary.h"
 #include "kmeans.cuh"
+#include "tuning.h"
 
 #include <algorithm>
 #include <chrono>
@@ -308,7 +309,8 @@ uint32_t Vocabulary::lookup(const uint8_t* devDesc, uint64_t n, uint32_t* devLea
         if (algo == kLookupSimtF32) throw Error(kUnsupported, "the FP32 SIMT lookup reads uint8 centers");
         return lookupFloat(devDesc, n, devLeaf, stream);
     }
-    if (algo == kLookupAuto) algo = kLookupTensorU8;
+    if (algo == kLookupAuto)
+        algo = tunedValue(kTuneLookupSchedule, mB, mL, n) == 2 ? kLookupTensorU8Ring : kLookupTensorU8;
     LookupScratch s{};
     if (algo == kLookupSimtF32) {
         s.err = mErrors.as<DeviceErrors>();

@@ -21,7 +21,9 @@ def _clean():
 
 
 def test_scatter_rows_candidates_are_exact(oracle):
-    B, L = 16, 4
+    """B=10, L=6: the regroup after the second pass has 10,000 bins, which takes the scatter
+    whose rows per thread are tuned."""
+    B, L = 10, 6
     centers, masks, weights = random_tree(B, L, seed=91)
     voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
     n = 300_007
@@ -33,6 +35,11 @@ def test_scatter_rows_candidates_are_exact(oracle):
         got = voc.lookup(desc, algo="tensor_u8")
         torch.cuda.synchronize()
         assert np.array_equal(got.cpu().numpy().view(np.uint32), want), rows
+    for sched in at.CANDIDATES["lookup_schedule"]:
+        at.set_value("lookup_schedule", B, L, at.bucket(n), sched)
+        got = voc.lookup(desc)  # algo "auto" runs the tuned schedule
+        torch.cuda.synchronize()
+        assert np.array_equal(got.cpu().numpy().view(np.uint32), want), sched
 
 
 @pytest.mark.parametrize("float_centers", [False, True])
@@ -60,9 +67,10 @@ def test_tuning_records_the_fastest_and_applies_it(tmp_path):
     voc = rbw.build_vocabulary(train, B, nb_doc=100, nb_levels=L, init="kmeans++", seed=1, max_iterations=4)
     desc = sift_like(1_000_000, seed=95, device="cuda")
     e2 = t.tune_lookup(voc, desc)
-    assert at.get_value("scatter_rows", B, L, desc.shape[0]) == e2["value"]
+    assert e2["value"] in at.CANDIDATES["lookup_schedule"]
+    assert at.get_value("lookup_schedule", B, L, desc.shape[0]) == e2["value"]
     t.save()
     at.clear()
     t2 = at.Autotuner.for_current_device(t.path)
     assert t2.load() and t2.apply() == 2
-    assert at.get_value("scatter_rows", B, L, desc.shape[0]) == e2["value"]
+    assert at.get_value("lookup_schedule", B, L, desc.shape[0]) == e2["value"]
