@@ -37,10 +37,8 @@ constexpr uint32_t kNodeBytes = kMaxBranch * kDims;   // 2 KB: one node's 16 cen
 constexpr uint32_t kBBlockBytes = kNodeBytes * 17;    // node + up to 16 children
 constexpr uint32_t kTeamWarps = 4;                    // epilogue team: one warp per TMEM lane quarter
 constexpr uint32_t kIssuer1Warp = 2 + 2 * kTeamWarps;        // second MMA issuer, after the teams
-constexpr uint32_t kProducer1Warp = kIssuer1Warp + 1;        // second gather producer (pair schedule)
-// producer, two MMA issuers, two epilogue teams, a second producer for the gathered passes
-constexpr uint32_t kTcThreads = 32 * (4 + 2 * kTeamWarps);
-constexpr uint32_t kRingThreads = 32 * (4 + 2 * kTeamWarps); // ring schedule: three MMA issuers
+constexpr uint32_t kTcThreads = 32 * (3 + 2 * kTeamWarps); // TMA, two MMA issuers, two epilogue teams
+constexpr uint32_t kRingThreads = kTcThreads + 32;          // ring schedule: three MMA issuers
 constexpr uint32_t kSmemHistMax = 1024;
 constexpr uint32_t kRegroupCtas = 148;                // regroup kernels' CTAs (one per SM on 148 SMs)
 // Two accumulator buffers of 256 columns; tile t uses buffer t & 1.  Its level-2p MMA (16
@@ -288,20 +286,11 @@ __device__ __forceinline__ void emitRow(TcSmem& S, const PassParams& p, bool sme
 // ------------------------------------------------------------------ producer warp
 // Stages the CTA's tiles [t0, t0 + nT) into the kStages shared-memory slots (arrival on aFull[s],
 // waits on aEmpty[s]) and each centre group's block (node + children, bFull / bEmpty).
-// kHalves = 2: in gathered passes two producer warps share each tile, warp `half` copying rows
-// [64 half, 64 half + 64) and arriving once on aFull (count 2); half 0 alone loads the centre
-// blocks and runs the TMA loads of the first pass.
-template <uint32_t kHalves>
 __device__ __forceinline__ void passProducer(TcSmem& S, const PassParams& p, const CUtensorMap* tmapTile,
-                                             uint32_t t0, uint32_t nT, uint32_t lane, volatile uint32_t* abortFlag,
-                                             uint32_t half)
+                                             uint32_t t0, uint32_t nT, uint32_t lane, volatile uint32_t* abortFlag)
 {
-    constexpr uint32_t kRows = kTileRows / kHalves;  // rows of a tile this warp gathers
-    constexpr uint32_t kGroupRows = kRows / 4;       // rows per group of eight lanes
-    const uint32_t rowBase = half * kRows;
     const bool two = p.twoLevels != 0;
     const bool gather = p.perm != nullptr;
-    const bool lead = half == 0;
     // First pass: one TMA tiled load (128 rows, 128-byte swizzle) per tile.
     // Later passes: the tile's 128 rows are gathered with 16-byte cp.async (lane q copies chunk
     // q % 8 of rows 32 (q / 8) + k) into the same swizzled layout, kGatherDepth tiles in flight.
@@ -314,8 +303,8 @@ __device__ __forceinline__ void passProducer(TcSmem& S, const PassParams& p, con
         if (i < nT) {
             const TileInfo ti = tileAtSmem(S, p, t0, i);
 #pragma unroll
-            for (uint32_t j = 0; j < kRows / 32; j++) {
-                const uint32_t rr = rowBase + (kRows / 32) * lane + j;
+            for (uint32_t j = 0; j < 4; j++) {
+                const uint32_t rr = 4 * lane + j;
                 cpAsync4(&S.idx[i % kIdxSlots][rr], p.perm + ti.start + (rr < ti.count ? rr : 0u));
             }
         }
@@ -344,7 +333,7 @@ __device__ __forceinline__ void passProducer(TcSmem& S, const PassParams& p, con
             if (i >= kGatherDepth) publishUpTo(i - kGatherDepth + 1);
         }
         bool ok = true;
-        if (lead && ti.group != prevGroup) {
+        if (ti.group != prevGroup) {
             // A slot is released only after the MMA and epilogue are done with tile i-2 or
             // earlier, so every gathered tile must be published before waiting for it.
             if (gather) {
@@ -389,22 +378,22 @@ __device__ __forceinline__ void passProducer(TcSmem& S, const PassParams& p, con
             __syncwarp();
             // All indices are read before the first copy: the copies are ordered with shared
             // memory accesses, so reads interleaved with them would each wait in turn.
-            // Lane group g = lane / 8 copies rows rowBase + kGroupRows g .. + kGroupRows - 1,
-            // whose indices it reads with 16-byte loads.
+            // Lane group g = lane / 8 copies rows 32 g .. 32 g + 31, whose indices it reads
+            // with eight 16-byte loads.
             const int32_t* ring = &S.idx[i % kIdxSlots][0];
             const uint32_t c = lane & 7u;
-            uint32_t rowIdx[kGroupRows];
+            uint32_t rowIdx[kTileRows / 4];
 #pragma unroll
-            for (uint32_t k = 0; k < kGroupRows / 4; k++) {
-                const int4 v = *reinterpret_cast<const int4*>(ring + rowBase + kGroupRows * (lane >> 3) + 4u * k);
+            for (uint32_t k = 0; k < kTileRows / 16; k++) {
+                const int4 v = *reinterpret_cast<const int4*>(ring + 32u * (lane >> 3) + 4u * k);
                 rowIdx[4 * k] = static_cast<uint32_t>(v.x);
                 rowIdx[4 * k + 1] = static_cast<uint32_t>(v.y);
                 rowIdx[4 * k + 2] = static_cast<uint32_t>(v.z);
                 rowIdx[4 * k + 3] = static_cast<uint32_t>(v.w);
             }
 #pragma unroll
-            for (uint32_t k = 0; k < kGroupRows; k++) {
-                const uint32_t tr = rowBase + kGroupRows * (lane >> 3) + k; // row within the tile
+            for (uint32_t k = 0; k < kTileRows / 4; k++) {
+                const uint32_t tr = 32u * (lane >> 3) + k; // row within the tile
                 cpAsync16(S.a[s] + tr * kDims + ((c ^ (tr & 7u)) << 4), p.desc + uint64_t(rowIdx[k]) * kDims + (c << 4));
             }
             copyIdx(i + kGatherDepth);
@@ -453,7 +442,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < kStages; s++) {
-            mbarInit(&S.aFull[s], gather ? 2u : 1u); // gathered passes: both producers
+            mbarInit(&S.aFull[s], 1);
             // kWarpNode: the children MMA's commit (two levels) and the four warps of the team
             mbarInit(&S.aEmpty[s], kWarpNode ? (two ? 1u : 0u) + kTeamWarps : 1u);
         }
@@ -486,9 +475,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tcFenceAfter();
     const uint32_t tmem = S.tmemBase;
     if (nT > 0 && warp == 0) {
-        passProducer<2>(S, p, &tmapTile, t0, nT, lane, abortFlag, 0);
-    } else if (nT > 0 && warp == kProducer1Warp && gather) {
-        passProducer<2>(S, p, &tmapTile, t0, nT, lane, abortFlag, 1);
+        passProducer(S, p, &tmapTile, t0, nT, lane, abortFlag);
     } else if (nT > 0 && (warp == 1 || warp == kIssuer1Warp)) {
         // ------------------------------------------------------------ MMA issuers (one thread each)
         // Issuer j (warp 1 for j = 0, warp kIssuer1Warp for j = 1) issues the MMAs of the tiles
@@ -751,7 +738,7 @@ __global__ void __launch_bounds__(kRingThreads, 1)
     // issuer role: 0 node level (warp 1), 1 + h children half h (warps 10 and 11)
     const uint32_t role = warp == 1 ? 0u : warp == kIssuer1Warp ? 1u : warp == kIssuer1Warp + 1 ? 2u : 99u;
     if (nT > 0 && warp == 0) {
-        passProducer<1>(S, p, &tmapTile, t0, nT, lane, abortFlag, 0);
+        passProducer(S, p, &tmapTile, t0, nT, lane, abortFlag);
     } else if (nT > 0 && role < issuers) {
         // ------------------------------------------------------------ MMA issuers (one thread each)
         if (lane == 0) {
