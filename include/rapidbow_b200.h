@@ -373,7 +373,7 @@ RBW_API int rbw_idf_weights(uint32_t nb_doc, const uint32_t* occ, uint64_t n, fl
  * (parameter, branch factor, tree levels, descriptor-count bucket = floor(log2(n))); levels 0
  * matches any depth.  Unset entries use the defaults. */
 enum {
-    RBW_TUNE_ASSIGN_CTAS_PER_SM = 0,     /* uint8 k-means assign: CTAs per SM, 1..6 (default 6) */
+    RBW_TUNE_ASSIGN_CTAS_PER_SM = 0,     /* uint8 k-means assign: CTAs per SM, 1..8 (default 6) */
     RBW_TUNE_ASSIGN_F32_CTAS_PER_SM = 1, /* float-center assign: CTAs per SM, 1..3 (default 3) */
     RBW_TUNE_SCATTER_ROWS = 2,           /* lookup regroup: rows per thread, 8, 16 or 32 (default 16) */
     RBW_TUNE_DB_SHARD_TABLES = 3,        /* DataBase inverted file, keyed by documents instead of

@@ -5,7 +5,7 @@ candidates of each tunable parameter are timed on the caller's own workload (CUD
 the library's kernels, rbw_timing_*) and the fastest is kept, per (parameter, branch factor,
 tree levels, descriptor-count bucket = floor(log2(n))):
 
-    assign_ctas_per_sm      uint8 k-means assign, CTAs per SM: 2..6         (default 6)
+    assign_ctas_per_sm      uint8 k-means assign, CTAs per SM: 2..8         (default 6)
     assign_f32_ctas_per_sm  float-center assign, CTAs per SM: 1..3          (default 3)
     scatter_rows            lookup regroup scatter of more than 1,024 bins, rows per thread:
                             8|16|32 (default 16)
@@ -36,7 +36,7 @@ PARAMS = {"assign_ctas_per_sm": 0, "assign_f32_ctas_per_sm": 1, "scatter_rows": 
           "lookup_schedule": 4}
 DEFAULTS = {"assign_ctas_per_sm": 6, "assign_f32_ctas_per_sm": 3, "scatter_rows": 16, "db_shard_tables": 1,
             "lookup_schedule": 1}
-CANDIDATES = {"assign_ctas_per_sm": (2, 3, 4, 5, 6), "assign_f32_ctas_per_sm": (1, 2, 3), "scatter_rows": (8, 16, 32),
+CANDIDATES = {"assign_ctas_per_sm": (2, 3, 4, 5, 6, 7, 8), "assign_f32_ctas_per_sm": (1, 2, 3), "scatter_rows": (8, 16, 32),
               "db_shard_tables": (1, 2), "lookup_schedule": (1, 2)}
 FORMAT = "rapidbow_b200 tuning cache"
 VERSION = 1

@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint
 constexpr uint32_t kAssignThreads = 128;
 constexpr uint32_t kAssignRows = 128;
 constexpr uint32_t kAssignTmemCols = 32; // the smallest allocation; the MMA writes 16 columns
-constexpr uint32_t kAssignCtasPerSm = 6; // by registers (<= 80) and shared memory; 192 TMEM columns
+constexpr uint32_t kAssignCtasPerSm = 8; // by registers (<= 64) and shared memory; 256 TMEM columns
 
 struct AssignSmem {
     uint8_t tile[kAssignRows * kDims];   // member rows, 128-byte swizzle (1024-byte aligned)

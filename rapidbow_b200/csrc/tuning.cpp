@@ -15,7 +15,7 @@ std::map<Key, uint32_t> gTable;
 bool valid(TuneParam p, uint32_t v)
 {
     switch (p) {
-    case kTuneAssignCtasPerSm: return v >= 1 && v <= 6;
+    case kTuneAssignCtasPerSm: return v >= 1 && v <= 8;
     case kTuneAssignFCtasPerSm: return v >= 1 && v <= 3;
     case kTuneScatterRows: return v == 8 || v == 16 || v == 32;
     case kTuneDbShardTables: return v == 1 || v == 2;

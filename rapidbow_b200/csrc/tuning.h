@@ -7,7 +7,7 @@
 namespace rbw {
 
 enum TuneParam : uint32_t {
-    kTuneAssignCtasPerSm = 0,  // uint8 k-means assign: resident CTAs per SM, 1..6 (default 6)
+    kTuneAssignCtasPerSm = 0,  // uint8 k-means assign: resident CTAs per SM, 1..8 (default 6)
     kTuneAssignFCtasPerSm = 1, // float-center assign: resident CTAs per SM, 1..3 (default 3)
     kTuneScatterRows = 2,      // lookup regroup scatter: rows per thread, 8 | 16 | 32 (default 16)
     kTuneDbShardTables = 3,    // inverted file: 1 one CSR per 2,560-document shard while small (default), 2 one CSR
