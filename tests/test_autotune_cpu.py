@@ -30,7 +30,7 @@ def test_choose_fastest_smallest_on_ties():
 def test_tune_records_applies_and_round_trips(tmp_path):
     path = str(tmp_path / "cache.json")
     t = at.Autotuner("NVIDIA B200", 148, path)
-    fake = {2: 1.9, 3: 1.2, 4: 1.1, 5: 1.3, 6: 1.4}
+    fake = {2: 1.9, 3: 1.2, 4: 1.1, 5: 1.3, 6: 1.4, 7: 1.5, 8: 1.6}
     calls = []
 
     def measure():
@@ -39,7 +39,7 @@ def test_tune_records_applies_and_round_trips(tmp_path):
         return fake[v]
 
     e = t.tune("assign_ctas_per_sm", 10, 0, 10_000_000, measure)
-    assert calls == [2, 3, 4, 5, 6]
+    assert calls == [2, 3, 4, 5, 6, 7, 8]
     assert e["value"] == 4 and e["bucket"] == 23 and e["default_ms"] == 1.4
     assert at.get_value("assign_ctas_per_sm", 10, 0, 9_000_000) == 4       # same bucket
     assert at.get_value("assign_ctas_per_sm", 10, 0, 1 << 24) == 6          # next bucket: default
