@@ -67,7 +67,7 @@ def test_library_rejects_bad_values():
         at.set_value("scatter_rows", 16, 4, 20, 12)
     assert e.value.status == rbw.RBW_ERR_INVALID_ARG
     with pytest.raises(rbw.RbwError):
-        at.set_value("assign_ctas_per_sm", 16, 0, 20, 7)
+        at.set_value("assign_ctas_per_sm", 16, 0, 20, 9)
     with pytest.raises(rbw.RbwError):
         at.set_value("assign_f32_ctas_per_sm", 1, 0, 20, 2)  # branch factor out of range
     at.set_value("scatter_rows", 16, 4, 20, 32)
