@@ -602,6 +602,9 @@ def build_bench(args, dev, rank):
                                                           init="kmeans++", seed=7, max_iterations=10)
             tune = {"param": e["param"], "value": e["value"], "tuned_assign_ms": e["ms"],
                     "default_assign_ms": e["default_ms"]}
+            if "sums" in e:
+                tune["sums"] = {"value": e["sums"]["value"], "candidates_ms": e["sums"]["candidates"],
+                                "note": "1 = shared-memory atomics, 2 = a second MMA per tile"}
         rbw.timing_reset()
         rbw.timing_enable(True)
         voc2, s2 = timed_build(c2, 10, 6, 3, float_centers=fl)

@@ -11,6 +11,8 @@ tree levels, descriptor-count bucket = floor(log2(n))):
                             8|16|32 (default 16)
     lookup_schedule         tensor-core lookup schedule of algo "auto": 1 level pairs in two
                             accumulator buffers, 2 the three-slot ring (default 1)
+    assign_sums             uint8 k-means center sums: 1 shared atomics, 2 a second MMA per
+                            tile (default 1; with 2 at most 5 CTAs per SM)
     db_shard_tables         DataBase inverted file: 1 one CSR per 2,560-document shard while
                             small, 2 one CSR (default 1; its bucket counts documents)
 
@@ -33,11 +35,11 @@ import numpy as np
 from . import _check, load_library
 
 PARAMS = {"assign_ctas_per_sm": 0, "assign_f32_ctas_per_sm": 1, "scatter_rows": 2, "db_shard_tables": 3,
-          "lookup_schedule": 4}
+          "lookup_schedule": 4, "assign_sums": 5}
 DEFAULTS = {"assign_ctas_per_sm": 6, "assign_f32_ctas_per_sm": 3, "scatter_rows": 16, "db_shard_tables": 1,
-            "lookup_schedule": 1}
+            "lookup_schedule": 1, "assign_sums": 1}
 CANDIDATES = {"assign_ctas_per_sm": (2, 3, 4, 5, 6, 7, 8), "assign_f32_ctas_per_sm": (1, 2, 3), "scatter_rows": (8, 16, 32),
-              "db_shard_tables": (1, 2), "lookup_schedule": (1, 2)}
+              "db_shard_tables": (1, 2), "lookup_schedule": (1, 2), "assign_sums": (1, 2)}
 FORMAT = "rapidbow_b200 tuning cache"
 VERSION = 1
 
@@ -153,11 +155,12 @@ class Autotuner:
         return self.record(param, B, L, n, timings)
 
     def tune_build(self, desc, B: int, L: int, float_centers: bool = False, repeats: int = 2, **build_kw) -> dict:
-        """Tunes the assign grid on a build of `desc` (CUDA uint8 [n, 128]); the build itself is
-        the workload, timed by the library's assign-kernel events."""
+        """Tunes the assign kernel on a build of `desc` (CUDA uint8 [n, 128]); the build itself is
+        the workload, timed by the library's assign-kernel events.  uint8 centers: the center sums
+        (shared atomics or the tensor core) first, then the CTAs per SM for the chosen sums;
+        returns the second entry, with the first under "sums"."""
         from . import build_vocabulary, timing_enable, timing_read, timing_reset
 
-        param = "assign_f32_ctas_per_sm" if float_centers else "assign_ctas_per_sm"
         n = desc.shape[0]
 
         def measure() -> float:
@@ -169,7 +172,12 @@ class Autotuner:
             timing_enable(False)
             return timing_read("kmeans_assign")[0] / repeats
 
-        return self.tune(param, B, 0, n, measure)
+        if float_centers:
+            return self.tune("assign_f32_ctas_per_sm", B, 0, n, measure)
+        sums = self.tune("assign_sums", B, 0, n, measure)
+        e = self.tune("assign_ctas_per_sm", B, 0, n, measure,
+                      candidates=[v for v in CANDIDATES["assign_ctas_per_sm"] if sums["value"] == 1 or v <= 5])
+        return dict(e, sums=sums)
 
     def tune_lookup(self, voc, desc, repeats: int = 3) -> dict:
         """Tunes the tensor-core schedule of algo "auto" on lookups of `desc` through `voc`, timed

@@ -501,6 +501,249 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignCtasPerSm) assignKernel
     }
 }
 
+// ------------------------------------------------------------------ assign, sums on the tensor core
+// The same assignment as assignKernel; the center sums come from a second MMA per tile instead of
+// 128 shared atomics per member: D[dim][center] += XT[dim][member] * OH[center][member], with XT
+// the tile transposed in shared memory (4 x 4 byte blocks through byte permutes) and OH the
+// one-hot of the members' centers built from ballots.  Both operands are K-major with K =
+// members, u8 x u8 -> s32 (exact); D lives in TMEM columns [16, 32) and accumulates over the
+// node's tiles in this CTA, read and written out when the CTA moves to another node (or every
+// kTsFlushTiles tiles, which keeps each s32 below 2^31: 65,536 x 128 x 255 < 2^31).
+constexpr uint32_t kAssignTsCtasPerSm = 5;     // by shared memory (~38 KB each)
+constexpr uint32_t kTsFlushTiles = 65536;
+
+struct AssignTsSmem {
+    uint8_t tile[kAssignRows * kDims];   // member rows, K-major (dims), 128-byte swizzle
+    uint8_t xt[kDims * kAssignRows];     // the rows transposed: [dim][member], same layout
+    uint8_t oh[kMaxBranch * kAssignRows]; // [center][member]: 1 where the member chose the center
+    uint8_t cen[kMaxBranch * kDims];     // node centers
+    int32_t cn[kMaxBranch];
+    uint32_t cnt[kMaxBranch];
+    uint64_t mmaBar, sumBar;
+    uint32_t tmemBase;
+    uint32_t chg;
+    uint32_t abortFlag;
+};
+constexpr size_t kAssignTsSmemBytes = sizeof(AssignTsSmem) + 1024;
+
+// Byte (row, col) of a 128-column, 128-byte-swizzled K-major operand.
+__device__ __forceinline__ uint32_t sw128(uint32_t row, uint32_t col)
+{
+    return row * 128u + ((((col >> 4) ^ row) & 7u) << 4) + (col & 15u);
+}
+
+__global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
+    assignKernelTs(KMeansLevel lv, const NodeTile* tiles, const uint32_t* nTilesDev)
+{
+    extern __shared__ uint8_t smemRaw[];
+    AssignTsSmem& S =
+        *reinterpret_cast<AssignTsSmem*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+    const uint32_t tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+    const uint32_t T = *nTilesDev;
+    const uint32_t t0 = static_cast<uint32_t>(uint64_t(T) * blockIdx.x / gridDim.x);
+    const uint32_t t1 = static_cast<uint32_t>(uint64_t(T) * (blockIdx.x + 1) / gridDim.x);
+    volatile uint32_t* abortFlag = &S.abortFlag;
+    if (tid == 0) {
+        mbarInit(&S.mmaBar, 1);
+        mbarInit(&S.sumBar, 1);
+        S.abortFlag = 0;
+        fenceMbarInit();
+    }
+    if (warp == 0) {
+        tmemAlloc(&S.tmemBase, kAssignTmemCols);
+        tmemRelinquish();
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tmem = S.tmemBase;
+    uint32_t curNode = 0xFFFFFFFFu, phase = 0, sumPhase = 0, accTiles = 0;
+    bool curExclusive = false, sumInFlight = false, ok = true;
+    auto waitSums = [&]() {
+        if (!sumInFlight) return;
+        ok = ok && mbarWait(&S.sumBar, sumPhase, abortFlag, lv.err, 42);
+        sumPhase ^= 1u;
+        sumInFlight = false;
+        tcFenceAfter();
+    };
+    // writes the node's partial sums (TMEM), counts and change count
+    auto flush = [&]() {
+        __syncthreads();
+        if (curNode != 0xFFFFFFFFu) {
+            if (accTiles > 0) {
+                waitSums();
+                uint32_t r[16];
+                tmemLoad16(tmem + 16u + ((warp * 32u) << 16), r); // lane = dimension tid
+                tmemWaitTie(r);
+                tcFenceBefore();
+#pragma unroll
+                for (uint32_t b = 0; b < kMaxBranch; b++) {
+                    if (r[b] == 0) continue;
+                    unsigned long long* dst = lv.sums + (uint64_t(curNode) * kMaxBranch + b) * kDims + tid;
+                    if (curExclusive) *dst = r[b];
+                    else atomicAdd(dst, (unsigned long long)r[b]);
+                }
+            }
+            if (tid < kMaxBranch && S.cnt[tid]) {
+                uint32_t* dst = lv.counts + uint64_t(curNode) * kMaxBranch + tid;
+                if (curExclusive) *dst = S.cnt[tid];
+                else atomicAdd(dst, S.cnt[tid]);
+            }
+            if (tid == 0 && S.chg) {
+                if (curExclusive) lv.changed[curNode] = S.chg;
+                else atomicAdd(lv.changed + curNode, S.chg);
+            }
+        }
+        accTiles = 0;
+        __syncthreads();
+    };
+    for (uint32_t t = t0; ok && t < t1; t++) {
+        const NodeTile ti = tiles[t];
+        if (lv.lastChanged[ti.node] == 0) continue; // frozen node (kmeans.cu:238-240)
+        if (ti.node != curNode) {
+            flush();
+            curNode = ti.node;
+            curExclusive = ti.first >= t0 && uint64_t(ti.first) + (lv.nodeCnt[curNode] + kAssignRows - 1) / kAssignRows <= t1;
+            {
+                const uint32_t b = tid / 8, c = tid % 8;
+                const uint4 v = reinterpret_cast<const uint4*>(lv.centers + (uint64_t(curNode) * kMaxBranch + b) * kDims)[c];
+                *reinterpret_cast<uint4*>(S.cen + b * kDims + ((c ^ (b & 7u)) << 4)) = v;
+            }
+            if (tid < kMaxBranch) {
+                S.cn[tid] = lv.cnorm[uint64_t(curNode) * kMaxBranch + tid];
+                S.cnt[tid] = 0;
+            }
+            if (tid == 0) S.chg = 0;
+        } else if (accTiles == kTsFlushTiles) {
+            // keep each s32 sum below 2^31: add this node's partial results to global memory and
+            // go on from zero (its later flushes add too)
+            curExclusive = false;
+            flush();
+            if (tid < kMaxBranch) S.cnt[tid] = 0;
+            if (tid == 0) S.chg = 0;
+            __syncthreads();
+        }
+        {
+            // eight threads per row, 16 rows per round; rows past the tile's count repeat its
+            // first member (their results are not used)
+            const uint32_t c = tid % 8;
+            uint32_t m[kAssignRows / 16];
+#pragma unroll
+            for (uint32_t k = 0; k < kAssignRows / 16; k++) {
+                const uint32_t row = 16u * k + tid / 8;
+                m[k] = lv.members[uint64_t(ti.start) + (row < ti.count ? row : 0u)];
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kAssignRows / 16; k++) {
+                const uint32_t row = 16u * k + tid / 8;
+                cpAsync16(S.tile + row * kDims + ((c ^ (row & 7u)) << 4), lv.desc + uint64_t(m[k]) * kDims + (c << 4));
+            }
+            cpAsyncCommit();
+            cpAsyncWait<0>();
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            tcFenceAfter();
+            const uint32_t aBase = smemAddr(S.tile), bBase = smemAddr(S.cen);
+#pragma unroll
+            for (uint32_t q4 = 0; q4 < 4; q4++)
+                mmaU8(tmem, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4), idescU8(16),
+                      q4 > 0 ? 1u : 0u);
+            mmaCommit(&S.mmaBar);
+        }
+        if (!mbarWait(&S.mmaBar, phase, abortFlag, lv.err, 41)) {
+            ok = false;
+            break;
+        }
+        phase ^= 1u;
+        tcFenceAfter();
+        const uint32_t row = tid;
+        uint32_t r[16];
+        tmemLoad16(tmem + ((warp * 32u) << 16), r);
+        tmemWaitTie(r);
+        tcFenceBefore();
+        int32_t best = S.cn[0] - 2 * static_cast<int32_t>(r[0]);
+        uint32_t bi = 0;
+#pragma unroll
+        for (uint32_t b = 1; b < kMaxBranch; b++) {
+            const int32_t sc = S.cn[b] - 2 * static_cast<int32_t>(r[b]);
+            if (sc < best) {
+                best = sc;
+                bi = b;
+            }
+        }
+        const bool valid = row < ti.count;
+        if (valid) {
+            const uint64_t at = uint64_t(ti.start) + row;
+            if (lv.assign[at] != bi) atomicAdd(&S.chg, 1u);
+            lv.assign[at] = static_cast<uint8_t>(bi);
+            atomicAdd(&S.cnt[bi], 1u);
+        }
+        // the previous tile's sums MMA must be done reading xt and oh before they are rewritten
+        waitSums();
+        if (!ok) break;
+        // one-hot: lane c writes row c's 32 bytes of this warp's members (bit i = member 32 w + i)
+        uint32_t mine = 0;
+#pragma unroll
+        for (uint32_t c = 0; c < kMaxBranch; c++) {
+            const uint32_t bits = __ballot_sync(0xFFFFFFFFu, valid && bi == c);
+            if (lane == c) mine = bits;
+        }
+        if (lane < kMaxBranch) {
+#pragma unroll
+            for (uint32_t half = 0; half < 2; half++) {
+                uint32_t w4[4];
+#pragma unroll
+                for (uint32_t q = 0; q < 4; q++) {
+                    const uint32_t nib = (mine >> (16u * half + 4u * q)) & 0xFu;
+                    w4[q] = (nib & 1u) | ((nib & 2u) << 7) | ((nib & 4u) << 14) | ((nib & 8u) << 21);
+                }
+                const uint32_t col = 32u * warp + 16u * half;
+                *reinterpret_cast<uint4*>(S.oh + sw128(lane, col)) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+            }
+        }
+        // transpose this warp's 32 rows into xt columns 32 w .. 32 w + 31, 4 x 4 byte blocks:
+        // lane = (dimension quad dq0 = lane / 8, member quad mq = lane % 8), eight dimension quads
+        {
+            const uint32_t m0 = 32u * warp + 4u * (lane & 7u);
+#pragma unroll
+            for (uint32_t k = 0; k < 8; k++) {
+                const uint32_t d0 = 4u * ((lane >> 3) + 4u * k);
+                const uint32_t w0 = *reinterpret_cast<const uint32_t*>(S.tile + sw128(m0, d0));
+                const uint32_t w1 = *reinterpret_cast<const uint32_t*>(S.tile + sw128(m0 + 1, d0));
+                const uint32_t w2 = *reinterpret_cast<const uint32_t*>(S.tile + sw128(m0 + 2, d0));
+                const uint32_t w3 = *reinterpret_cast<const uint32_t*>(S.tile + sw128(m0 + 3, d0));
+                const uint32_t a = __byte_perm(w0, w1, 0x5140), b = __byte_perm(w2, w3, 0x5140);
+                const uint32_t c = __byte_perm(w0, w1, 0x7362), d = __byte_perm(w2, w3, 0x7362);
+                *reinterpret_cast<uint32_t*>(S.xt + sw128(d0, m0)) = __byte_perm(a, b, 0x5410);
+                *reinterpret_cast<uint32_t*>(S.xt + sw128(d0 + 1, m0)) = __byte_perm(a, b, 0x7632);
+                *reinterpret_cast<uint32_t*>(S.xt + sw128(d0 + 2, m0)) = __byte_perm(c, d, 0x5410);
+                *reinterpret_cast<uint32_t*>(S.xt + sw128(d0 + 3, m0)) = __byte_perm(c, d, 0x7632);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads(); // xt, oh complete; the tile is rewritten by the next gather
+        if (tid == 0) {
+            tcFenceAfter();
+            const uint32_t aBase = smemAddr(S.xt), bBase = smemAddr(S.oh);
+#pragma unroll
+            for (uint32_t q4 = 0; q4 < 4; q4++)
+                mmaU8(tmem + 16u, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4), idescU8(16),
+                      (accTiles > 0 || q4 > 0) ? 1u : 0u);
+            mmaCommit(&S.sumBar);
+        }
+        sumInFlight = true;
+        accTiles++;
+    }
+    if (ok) flush();
+    else waitSums();
+    if (warp == 0) {
+        tcFenceAfter();
+        tmemDealloc(tmem, kAssignTmemCols);
+    }
+}
+
 // ------------------------------------------------------------------ regroup
 constexpr uint32_t kRegroupRows = 32;
 
@@ -637,10 +880,19 @@ void launchAssign(const KMeansLevel& lv, const NodeTile* tiles, const uint32_t* 
     // up to kAssignCtasPerSm CTAs per SM, the count the autotuner chose for this workload.
     static_assert(kAssignCtasPerSm * kAssignTmemCols <= 512, "TMEM columns of the resident CTAs");
     static_assert(kAssignCtasPerSm * kAssignSmemBytes <= 227 * 1024, "shared memory of the resident CTAs");
-    const uint32_t perSm = std::min(kAssignCtasPerSm, tunedValue(kTuneAssignCtasPerSm, lv.B, 0, lv.nbMembers));
+    static_assert(kAssignTsCtasPerSm * kAssignTsSmemBytes <= 227 * 1024, "shared memory of the resident CTAs");
+    const bool tensorSums = tunedValue(kTuneAssignSums, lv.B, 0, lv.nbMembers) == 2;
+    const uint32_t cap = tensorSums ? kAssignTsCtasPerSm : kAssignCtasPerSm;
+    const uint32_t perSm = std::min(cap, tunedValue(kTuneAssignCtasPerSm, lv.B, 0, lv.nbMembers));
     const uint32_t grid = std::max(1u, std::min<uint32_t>(maxTiles, static_cast<uint32_t>(sms) * perSm));
     ScopedKernelTimer timer(kTimedAssign, s);
-    assignKernel<<<grid, kAssignThreads, kAssignSmemBytes, s>>>(lv, tiles, nTilesDev);
+    if (tensorSums) {
+        static std::atomic<uint64_t> attr{0};
+        setMaxDynamicSmemOncePerDevice(reinterpret_cast<const void*>(assignKernelTs), int(kAssignTsSmemBytes), attr);
+        assignKernelTs<<<grid, kAssignThreads, kAssignTsSmemBytes, s>>>(lv, tiles, nTilesDev);
+    } else {
+        assignKernel<<<grid, kAssignThreads, kAssignSmemBytes, s>>>(lv, tiles, nTilesDev);
+    }
     RBW_CUDA(cudaGetLastError());
 }
 

@@ -20,6 +20,7 @@ bool valid(TuneParam p, uint32_t v)
     case kTuneScatterRows: return v == 8 || v == 16 || v == 32;
     case kTuneDbShardTables: return v == 1 || v == 2;
     case kTuneLookupSchedule: return v == 1 || v == 2;
+    case kTuneAssignSums: return v == 1 || v == 2;
     default: return false;
     }
 }
@@ -44,6 +45,7 @@ uint32_t tuneDefault(TuneParam p)
     case kTuneScatterRows: return 16;
     case kTuneDbShardTables: return 1;
     case kTuneLookupSchedule: return 1;
+    case kTuneAssignSums: return 1;
     default: return 0;
     }
 }

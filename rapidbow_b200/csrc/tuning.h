@@ -12,7 +12,8 @@ enum TuneParam : uint32_t {
     kTuneScatterRows = 2,      // lookup regroup scatter: rows per thread, 8 | 16 | 32 (default 16)
     kTuneDbShardTables = 3,    // inverted file: 1 one CSR per 2,560-document shard while small (default), 2 one CSR
     kTuneLookupSchedule = 4,   // tensor-core lookup of RBW_LOOKUP_AUTO: 1 pair schedule (default), 2 ring
-    kTuneParamCount = 5,
+    kTuneAssignSums = 5,       // uint8 k-means center sums: 1 shared atomics (default), 2 tensor core
+    kTuneParamCount = 6,
 };
 
 // floor(log2(max(n, 1))): workloads within a factor of two share an entry.

@@ -57,6 +57,26 @@ def test_assign_grid_candidates_give_identical_builds(float_centers):
         assert np.array_equal(c, trees[0][0]) and np.array_equal(w, trees[0][1])
 
 
+def test_tensor_core_sums_give_the_oracle_build(oracle):
+    """Center sums from the second MMA per tile (assign_sums = 2) equal the shared-atomic sums:
+    the IEEE-rounding build equals the oracle's byte for byte, on a one-node level of 150,000
+    members (a node spread over many CTAs) and on small nodes."""
+    from oracle.pyoracle import INIT_KMEANSPP
+
+    desc_t = sift_like(150_000, seed=96, n_components=4096, zipf=1.1, device="cuda")
+    desc = desc_t.cpu().numpy()
+    B, L = 10, 3
+    at.set_value("assign_sums", B, 0, at.bucket(desc.shape[0]), 2)
+    for ctas in (2, 5):
+        at.set_value("assign_ctas_per_sm", B, 0, at.bucket(desc.shape[0]), ctas)
+        voc = rbw.build_vocabulary(desc_t, B, nb_doc=100, nb_levels=L, init="kmeans++", seed=3, max_iterations=10,
+                                   ieee_division=True)
+        ref = oracle.build_vocabulary(desc, 100, B, L, max_iter=10, init=INIT_KMEANSPP, seed=3)
+        c, m, w = voc.tree()
+        assert np.array_equal(c, ref["centers"]) and np.array_equal(m, ref["masks"]), ctas
+        assert np.array_equal(w, ref["weights"]), ctas
+
+
 def test_tuning_records_the_fastest_and_applies_it(tmp_path):
     t = at.Autotuner.for_current_device(str(tmp_path / "tune.json"))
     B, L = 16, 4
