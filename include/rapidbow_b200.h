@@ -382,7 +382,7 @@ enum {
     RBW_TUNE_LOOKUP_SCHEDULE = 4,        /* the tensor-core schedule RBW_LOOKUP_AUTO runs: 1 level
                                             pairs in two buffers (default), 2 the three-slot ring */
     RBW_TUNE_ASSIGN_SUMS = 5             /* uint8 k-means center sums: 1 shared-memory atomics
-                                            (default), 2 a second MMA per tile (at most 5 CTAs/SM) */
+                                            (default), 2 a second MMA per tile (at most 4 CTAs/SM) */
 };
 /* value 0 removes the entry; RBW_ERR_INVALID_ARG for a value the parameter cannot take. */
 RBW_API int rbw_tuning_set(uint32_t param, uint32_t branch_factor, uint32_t nb_levels, uint32_t bucket,

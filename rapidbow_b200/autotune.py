@@ -12,7 +12,7 @@ tree levels, descriptor-count bucket = floor(log2(n))):
     lookup_schedule         tensor-core lookup schedule of algo "auto": 1 level pairs in two
                             accumulator buffers, 2 the three-slot ring (default 1)
     assign_sums             uint8 k-means center sums: 1 shared atomics, 2 a second MMA per
-                            tile (default 1; with 2 at most 5 CTAs per SM)
+                            tile (default 1; with 2 at most 4 CTAs per SM)
     db_shard_tables         DataBase inverted file: 1 one CSR per 2,560-document shard while
                             small, 2 one CSR (default 1; its bucket counts documents)
 
@@ -176,7 +176,7 @@ class Autotuner:
             return self.tune("assign_f32_ctas_per_sm", B, 0, n, measure)
         sums = self.tune("assign_sums", B, 0, n, measure)
         e = self.tune("assign_ctas_per_sm", B, 0, n, measure,
-                      candidates=[v for v in CANDIDATES["assign_ctas_per_sm"] if sums["value"] == 1 or v <= 5])
+                      candidates=[v for v in CANDIDATES["assign_ctas_per_sm"] if sums["value"] == 1 or v <= 4])
         return dict(e, sums=sums)
 
     def tune_lookup(self, voc, desc, repeats: int = 3) -> dict:

@@ -509,11 +509,12 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignCtasPerSm) assignKernel
 // members, u8 x u8 -> s32 (exact); D lives in TMEM columns [16, 32) and accumulates over the
 // node's tiles in this CTA, read and written out when the CTA moves to another node (or every
 // kTsFlushTiles tiles, which keeps each s32 below 2^31: 65,536 x 128 x 255 < 2^31).
-constexpr uint32_t kAssignTsCtasPerSm = 5;     // by shared memory (~38 KB each)
+constexpr uint32_t kAssignTsCtasPerSm = 4;     // by shared memory (~54 KB each)
 constexpr uint32_t kTsFlushTiles = 65536;
 
 struct AssignTsSmem {
-    uint8_t tile[kAssignRows * kDims];   // member rows, K-major (dims), 128-byte swizzle
+    uint8_t tile[2][kAssignRows * kDims]; // member rows, K-major (dims), 128-byte swizzle; the
+                                          // next tile's rows are gathered while this one is scored
     uint8_t xt[kDims * kAssignRows];     // the rows transposed: [dim][member], same layout
     uint8_t oh[kMaxBranch * kAssignRows]; // [center][member]: 1 where the member chose the center
     uint8_t cen[kMaxBranch * kDims];     // node centers
@@ -557,8 +558,26 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
     __syncthreads();
     tcFenceAfter();
     const uint32_t tmem = S.tmemBase;
-    uint32_t curNode = 0xFFFFFFFFu, phase = 0, sumPhase = 0, accTiles = 0;
-    bool curExclusive = false, sumInFlight = false, ok = true;
+    uint32_t curNode = 0xFFFFFFFFu, phase = 0, sumPhase = 0, accTiles = 0, buf = 0;
+    bool curExclusive = false, sumInFlight = false, ok = true, pendingNext = false;
+    // eight threads per row, 16 rows per round; rows past the tile's count repeat its first
+    // member (their results are not used); one copy group per tile
+    auto gatherTile = [&](uint32_t t, uint32_t b) {
+        const NodeTile tn = tiles[t];
+        const uint32_t c = tid % 8;
+        uint32_t m[kAssignRows / 16];
+#pragma unroll
+        for (uint32_t k = 0; k < kAssignRows / 16; k++) {
+            const uint32_t row = 16u * k + tid / 8;
+            m[k] = lv.members[uint64_t(tn.start) + (row < tn.count ? row : 0u)];
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kAssignRows / 16; k++) {
+            const uint32_t row = 16u * k + tid / 8;
+            cpAsync16(S.tile[b] + row * kDims + ((c ^ (row & 7u)) << 4), lv.desc + uint64_t(m[k]) * kDims + (c << 4));
+        }
+        cpAsyncCommit();
+    };
     auto waitSums = [&]() {
         if (!sumInFlight) return;
         ok = ok && mbarWait(&S.sumBar, sumPhase, abortFlag, lv.err, 42);
@@ -624,28 +643,24 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
             __syncthreads();
         }
         {
-            // eight threads per row, 16 rows per round; rows past the tile's count repeat its
-            // first member (their results are not used)
-            const uint32_t c = tid % 8;
-            uint32_t m[kAssignRows / 16];
-#pragma unroll
-            for (uint32_t k = 0; k < kAssignRows / 16; k++) {
-                const uint32_t row = 16u * k + tid / 8;
-                m[k] = lv.members[uint64_t(ti.start) + (row < ti.count ? row : 0u)];
+            // gather the next tile to be scored into the other buffer, then wait for this one's
+            if (!pendingNext) gatherTile(t, buf); // first tile, or after a skipped prefetch
+            uint32_t nt = t + 1;
+            while (nt < t1 && lv.lastChanged[tiles[nt].node] == 0) nt++;
+            if (nt < t1) {
+                gatherTile(nt, buf ^ 1u);
+                cpAsyncWait<1>();
+            } else {
+                cpAsyncWait<0>();
             }
-#pragma unroll
-            for (uint32_t k = 0; k < kAssignRows / 16; k++) {
-                const uint32_t row = 16u * k + tid / 8;
-                cpAsync16(S.tile + row * kDims + ((c ^ (row & 7u)) << 4), lv.desc + uint64_t(m[k]) * kDims + (c << 4));
-            }
-            cpAsyncCommit();
-            cpAsyncWait<0>();
+            pendingNext = nt < t1;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        const uint8_t* tileBuf = S.tile[buf];
         if (tid == 0) {
             tcFenceAfter();
-            const uint32_t aBase = smemAddr(S.tile), bBase = smemAddr(S.cen);
+            const uint32_t aBase = smemAddr(tileBuf), bBase = smemAddr(S.cen);
 #pragma unroll
             for (uint32_t q4 = 0; q4 < 4; q4++)
                 mmaU8(tmem, smemDescSw128(aBase + 32u * q4), smemDescSw128(bBase + 32u * q4), idescU8(16),
@@ -710,10 +725,10 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
 #pragma unroll
             for (uint32_t k = 0; k < 8; k++) {
                 const uint32_t d0 = 4u * ((lane >> 3) + 4u * k);
-                const uint32_t w0 = *reinterpret_cast<const uint32_t*>(S.tile + sw128(m0, d0));
-                const uint32_t w1 = *reinterpret_cast<const uint32_t*>(S.tile + sw128(m0 + 1, d0));
-                const uint32_t w2 = *reinterpret_cast<const uint32_t*>(S.tile + sw128(m0 + 2, d0));
-                const uint32_t w3 = *reinterpret_cast<const uint32_t*>(S.tile + sw128(m0 + 3, d0));
+                const uint32_t w0 = *reinterpret_cast<const uint32_t*>(tileBuf + sw128(m0, d0));
+                const uint32_t w1 = *reinterpret_cast<const uint32_t*>(tileBuf + sw128(m0 + 1, d0));
+                const uint32_t w2 = *reinterpret_cast<const uint32_t*>(tileBuf + sw128(m0 + 2, d0));
+                const uint32_t w3 = *reinterpret_cast<const uint32_t*>(tileBuf + sw128(m0 + 3, d0));
                 const uint32_t a = __byte_perm(w0, w1, 0x5140), b = __byte_perm(w2, w3, 0x5140);
                 const uint32_t c = __byte_perm(w0, w1, 0x7362), d = __byte_perm(w2, w3, 0x7362);
                 *reinterpret_cast<uint32_t*>(S.xt + sw128(d0, m0)) = __byte_perm(a, b, 0x5410);
@@ -735,7 +750,9 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
         }
         sumInFlight = true;
         accTiles++;
+        buf ^= 1u;
     }
+    cpAsyncWait<0>(); // a prefetch of a tile that was not scored (abort) must land before exit
     if (ok) flush();
     else waitSums();
     if (warp == 0) {
