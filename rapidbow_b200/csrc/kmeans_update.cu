@@ -12,22 +12,27 @@ namespace {
 
 __global__ void __launch_bounds__(256) updateKernel(KMeansLevel lv)
 {
-    __shared__ uint32_t ch;
+    __shared__ uint32_t ch, frozen;
     __shared__ uint32_t cnt[kMaxBranch];
     const uint32_t g = blockIdx.x;
     if (threadIdx.x == 0) {
         ch = lv.changed[g];
+        // A node frozen before this step was skipped by the assign: nothing was accumulated and
+        // every counter is already zero, so there is nothing to do.
+        frozen = lv.lastChanged[g] == 0 && ch == 0;
         lv.lastChanged[g] = ch;
         lv.changed[g] = 0;
         if (ch != 0) atomicAdd(lv.activeCount, 1u);
     }
     if (threadIdx.x < kMaxBranch) cnt[threadIdx.x] = lv.counts[uint64_t(g) * kMaxBranch + threadIdx.x];
     __syncthreads();
+    if (frozen) return;
     // Nodes with no change keep their centers (kmeans.cu:341-343); their accumulators are still
-    // cleared so the next level starts from zero.
+    // cleared so the next level starts from zero.  Centers b >= B have no members: their sums
+    // and counts stay zero.
     uint8_t* c = lv.centers + uint64_t(g) * kMaxBranch * kDims;
     unsigned long long* sums = lv.sums + uint64_t(g) * kMaxBranch * kDims;
-    for (uint32_t i = threadIdx.x; i < kMaxBranch * kDims; i += blockDim.x) {
+    for (uint32_t i = threadIdx.x; i < lv.B * kDims; i += blockDim.x) {
         const uint32_t b = i / kDims;
         const uint32_t n = cnt[b];
         if (ch != 0 && b < lv.B && n != 0) {
