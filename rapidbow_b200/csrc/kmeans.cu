@@ -511,6 +511,8 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignCtasPerSm) assignKernel
 // kTsFlushTiles tiles, which keeps each s32 below 2^31: 65,536 x 128 x 255 < 2^31).
 constexpr uint32_t kAssignTsCtasPerSm = 4;     // by shared memory (~54 KB each)
 constexpr uint32_t kTsFlushTiles = 65536;
+constexpr uint32_t kTsTileWindow = kAssignThreads; // one tile entry per thread per refill
+constexpr uint32_t kTsFrozen = 0x80000000u;
 
 struct AssignTsSmem {
     uint8_t tile[2][kAssignRows * kDims]; // member rows, K-major (dims), 128-byte swizzle; the
@@ -518,6 +520,8 @@ struct AssignTsSmem {
     uint8_t xt[kDims * kAssignRows];     // the rows transposed: [dim][member], same layout
     uint8_t oh[kMaxBranch * kAssignRows]; // [center][member]: 1 where the member chose the center
     uint8_t cen[kMaxBranch * kDims];     // node centers
+    NodeTile win[kTsTileWindow];         // tiles [winBase, winBase + kTsTileWindow) of the CTA's
+                                         // range, count | kTsFrozen for a frozen node
     int32_t cn[kMaxBranch];
     uint32_t cnt[kMaxBranch];
     uint64_t mmaBar, sumBar;
@@ -559,18 +563,43 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
     tcFenceAfter();
     const uint32_t tmem = S.tmemBase;
     uint32_t curNode = 0xFFFFFFFFu, phase = 0, sumPhase = 0, accTiles = 0, buf = 0;
-    bool curExclusive = false, sumInFlight = false, ok = true, pendingNext = false;
-    // eight threads per row, 16 rows per round; rows past the tile's count repeat its first
-    // member (their results are not used); one copy group per tile
-    auto gatherTile = [&](uint32_t t, uint32_t b) {
-        const NodeTile tn = tiles[t];
-        const uint32_t c = tid % 8;
-        uint32_t m[kAssignRows / 16];
+    bool curExclusive = false, sumInFlight = false, ok = true;
+    // The tile list and the frozen flags are read a window of kTsTileWindow tiles at a time (one
+    // load per thread, all in flight together), so that finding the next live tile costs no
+    // global round trip; the member indices of the next tile are loaded into registers one
+    // tile ahead of its row copies.  Every thread runs the same window refills (uniform).
+    uint32_t winBase = t0;
+    auto refill = [&](uint32_t base) {
+        __syncthreads(); // nobody reads the old window any more
+        if (base + tid < t1) {
+            NodeTile x = tiles[base + tid];
+            if (lv.lastChanged[x.node] == 0) x.count |= kTsFrozen; // frozen node (kmeans.cu:238-240)
+            S.win[tid] = x;
+        }
+        winBase = base;
+        __syncthreads();
+    };
+    auto entry = [&](uint32_t t) -> NodeTile {
+        if (t - winBase >= kTsTileWindow) refill(t);
+        return S.win[t - winBase];
+    };
+    // the first live tile at or after t, or t1
+    auto nextLive = [&](uint32_t t) -> uint32_t {
+        for (; t < t1; t++)
+            if (!(entry(t).count & kTsFrozen)) return t;
+        return t1;
+    };
+    auto loadIndices = [&](const NodeTile& tn, uint32_t (&m)[kAssignRows / 16]) {
 #pragma unroll
         for (uint32_t k = 0; k < kAssignRows / 16; k++) {
             const uint32_t row = 16u * k + tid / 8;
             m[k] = lv.members[uint64_t(tn.start) + (row < tn.count ? row : 0u)];
         }
+    };
+    // eight threads per row, 16 rows per round; rows past the tile's count repeat its first
+    // member (their results are not used); one copy group per tile
+    auto gatherRows = [&](const uint32_t (&m)[kAssignRows / 16], uint32_t b) {
+        const uint32_t c = tid % 8;
 #pragma unroll
         for (uint32_t k = 0; k < kAssignRows / 16; k++) {
             const uint32_t row = 16u * k + tid / 8;
@@ -616,9 +645,21 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
         accTiles = 0;
         __syncthreads();
     };
-    for (uint32_t t = t0; ok && t < t1; t++) {
-        const NodeTile ti = tiles[t];
-        if (lv.lastChanged[ti.node] == 0) continue; // frozen node (kmeans.cu:238-240)
+    if (t0 < t1) refill(t0);
+    uint32_t t = nextLive(t0);
+    NodeTile ti{}, tn1{};
+    uint32_t mNext[kAssignRows / 16];
+    if (t < t1) {
+        ti = entry(t);
+        loadIndices(ti, mNext);
+        gatherRows(mNext, buf);
+    }
+    uint32_t n1 = t < t1 ? nextLive(t + 1) : t1;
+    if (n1 < t1) {
+        tn1 = entry(n1);
+        loadIndices(tn1, mNext);
+    }
+    while (ok && t < t1) {
         if (ti.node != curNode) {
             flush();
             curNode = ti.node;
@@ -642,19 +683,25 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
             if (tid == 0) S.chg = 0;
             __syncthreads();
         }
-        {
-            // gather the next tile to be scored into the other buffer, then wait for this one's
-            if (!pendingNext) gatherTile(t, buf); // first tile, or after a skipped prefetch
-            uint32_t nt = t + 1;
-            while (nt < t1 && lv.lastChanged[tiles[nt].node] == 0) nt++;
-            if (nt < t1) {
-                gatherTile(nt, buf ^ 1u);
-                cpAsyncWait<1>();
-            } else {
-                cpAsyncWait<0>();
+        // the next live tile's rows go into the other buffer (its indices were loaded one tile
+        // ago), the indices of the one after it into registers; then this tile's rows must be in
+        uint32_t n2 = t1;
+        NodeTile tn2{};
+        if (n1 < t1) {
+            gatherRows(mNext, buf ^ 1u);
+            n2 = nextLive(n1 + 1);
+            if (n2 < t1) {
+                tn2 = entry(n2);
+                loadIndices(tn2, mNext);
             }
-            pendingNext = nt < t1;
+            cpAsyncWait<1>();
+        } else {
+            cpAsyncWait<0>();
         }
+        const uint32_t row = tid;
+        const bool valid = row < ti.count;
+        const uint64_t at = uint64_t(ti.start) + row;
+        const uint32_t prevAssign = valid ? lv.assign[at] : 0u;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         const uint8_t* tileBuf = S.tile[buf];
@@ -673,7 +720,6 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
         }
         phase ^= 1u;
         tcFenceAfter();
-        const uint32_t row = tid;
         uint32_t r[16];
         tmemLoad16(tmem + ((warp * 32u) << 16), r);
         tmemWaitTie(r);
@@ -688,10 +734,8 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
                 bi = b;
             }
         }
-        const bool valid = row < ti.count;
         if (valid) {
-            const uint64_t at = uint64_t(ti.start) + row;
-            if (lv.assign[at] != bi) atomicAdd(&S.chg, 1u);
+            if (prevAssign != bi) atomicAdd(&S.chg, 1u);
             lv.assign[at] = static_cast<uint8_t>(bi);
             atomicAdd(&S.cnt[bi], 1u);
         }
@@ -751,6 +795,10 @@ __global__ void __launch_bounds__(kAssignThreads, kAssignTsCtasPerSm)
         sumInFlight = true;
         accTiles++;
         buf ^= 1u;
+        t = n1;
+        ti = tn1;
+        n1 = n2;
+        tn1 = tn2;
     }
     cpAsyncWait<0>(); // a prefetch of a tile that was not scored (abort) must land before exit
     if (ok) flush();

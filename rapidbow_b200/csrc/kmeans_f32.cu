@@ -106,11 +106,15 @@ constexpr uint32_t kAfThreads = 128;
 constexpr uint32_t kAfRows = 128;
 constexpr uint32_t kAfTmemCols = 32;
 constexpr uint32_t kAfCtasPerSm = 3;
+constexpr uint32_t kAfTileWindow = kAfThreads; // one tile entry per thread per refill
+constexpr uint32_t kAfFrozen = 0x80000000u;
 
 struct AssignFSmem {
     uint8_t a[2][kAfRows * 128];     // members as bf16, two K-blocks of 64 dims, 128-byte swizzle
     uint8_t b[2][32 * 128];          // the node's hi (rows 0-15) and lo (rows 16-31) centers
     uint8_t x8[kAfRows * kDims];     // members as uint8, row-major (sums and FP64 re-score)
+    NodeTile win[kAfTileWindow];     // tiles [winBase, winBase + kAfTileWindow) of the CTA's range,
+                                     // count | kAfFrozen for a frozen node
     uint32_t acc[kMaxBranch * kDims]; // center sums of the current node (accIndex layout)
     unsigned long long q[kMaxBranch];
     float cn[kMaxBranch];
@@ -205,9 +209,60 @@ __global__ void __launch_bounds__(kAfThreads, kAfCtasPerSm) assignKernelF(KMeans
         }
         __syncthreads();
     };
-    for (uint32_t t = t0; t < t1; t++) {
-        const NodeTile ti = tiles[t];
-        if (build && L0.lastChanged[ti.node] == 0) continue; // frozen node (kmeans.cu:238-240)
+    // The tile list and the frozen flags are read a window of kAfTileWindow tiles at a time (one
+    // load per thread, all in flight together), the member indices two tiles ahead and the member
+    // rows one tile ahead of their use, into registers, so that no tile waits on a chain of
+    // dependent global loads.  Every thread runs the same window refills (uniform).
+    uint32_t winBase = t0;
+    auto refill = [&](uint32_t base) {
+        __syncthreads(); // nobody reads the old window any more
+        if (base + tid < t1) {
+            NodeTile x = tiles[base + tid];
+            if (build && L0.lastChanged[x.node] == 0) x.count |= kAfFrozen; // frozen node (kmeans.cu:238-240)
+            S.win[tid] = x;
+        }
+        winBase = base;
+        __syncthreads();
+    };
+    auto entry = [&](uint32_t t) -> NodeTile {
+        if (t - winBase >= kAfTileWindow) refill(t);
+        return S.win[t - winBase];
+    };
+    auto nextLive = [&](uint32_t t) -> uint32_t {
+        for (; t < t1; t++)
+            if (!(entry(t).count & kAfFrozen)) return t;
+        return t1;
+    };
+    // rows past a tile's count repeat its first member (their results are not used)
+    auto loadIndices = [&](const NodeTile& tn, uint32_t (&m)[kAfRows / 16]) {
+#pragma unroll
+        for (uint32_t k = 0; k < kAfRows / 16; k++) {
+            const uint32_t row = 16u * k + tid / 8;
+            m[k] = L0.members[uint64_t(tn.start) + (row < tn.count ? row : 0u)];
+        }
+    };
+    const uint32_t c8 = tid % 8;
+    auto loadRows = [&](const uint32_t (&m)[kAfRows / 16], uint4 (&v)[kAfRows / 16]) {
+#pragma unroll
+        for (uint32_t k = 0; k < kAfRows / 16; k++)
+            v[k] = __ldg(reinterpret_cast<const uint4*>(L0.desc + uint64_t(m[k]) * kDims) + c8);
+    };
+    if (t0 < t1) refill(t0);
+    uint32_t t = nextLive(t0);
+    NodeTile ti{}, tn1{};
+    uint32_t mNext[kAfRows / 16];
+    uint4 v[kAfRows / 16];
+    if (t < t1) {
+        ti = entry(t);
+        loadIndices(ti, mNext);
+        loadRows(mNext, v);
+    }
+    uint32_t n1 = t < t1 ? nextLive(t + 1) : t1;
+    if (n1 < t1) {
+        tn1 = entry(n1);
+        loadIndices(tn1, mNext);
+    }
+    while (t < t1) {
         if (tid == 0) S.visited += ti.count;
         if (ti.node != curNode) {
             flush();
@@ -233,19 +288,7 @@ __global__ void __launch_bounds__(kAfThreads, kAfCtasPerSm) assignKernelF(KMeans
             // Eight threads per row, 16 rows per round: thread c8 = tid % 8 stages dims
             // 16 c8 .. 16 c8 + 15 of its row as uint8 and as bf16 (K-block c8 / 4, 16-byte chunks
             // 2 (c8 % 4) and 2 (c8 % 4) + 1 of the 128-byte row, swizzled by the row's low bits),
-            // and the eight threads add up the row's |x|^2.  Rows past the tile's count repeat its
-            // first member (their results are not used).
-            const uint32_t c8 = tid % 8;
-            uint32_t m[kAfRows / 16];
-#pragma unroll
-            for (uint32_t k = 0; k < kAfRows / 16; k++) {
-                const uint32_t row = 16u * k + tid / 8;
-                m[k] = L0.members[uint64_t(ti.start) + (row < ti.count ? row : 0u)];
-            }
-            uint4 v[kAfRows / 16];
-#pragma unroll
-            for (uint32_t k = 0; k < kAfRows / 16; k++)
-                v[k] = __ldg(reinterpret_cast<const uint4*>(L0.desc + uint64_t(m[k]) * kDims) + c8);
+            // and the eight threads add up the row's |x|^2.
 #pragma unroll
             for (uint32_t k = 0; k < kAfRows / 16; k++) {
                 const uint32_t row = 16u * k + tid / 8;
@@ -269,6 +312,22 @@ __global__ void __launch_bounds__(kAfThreads, kAfCtasPerSm) assignKernelF(KMeans
                 if (c8 == 0) S.xn[row] = xn;
             }
         }
+        // the next live tile's rows into registers (its indices were loaded one tile ago), the
+        // indices of the one after it; both land while this tile is scored
+        uint32_t n2 = t1;
+        NodeTile tn2{};
+        if (n1 < t1) {
+            loadRows(mNext, v);
+            n2 = nextLive(n1 + 1);
+            if (n2 < t1) {
+                tn2 = entry(n2);
+                loadIndices(tn2, mNext);
+            }
+        }
+        const uint32_t row = tid;
+        const bool valid = row < ti.count;
+        const uint64_t at = uint64_t(ti.start) + row;
+        const uint32_t prevAssign = build && valid ? L0.assign[at] : 0u; // lands during the MMA
         // generic-proxy shared-memory writes read by the tensor core
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -291,8 +350,6 @@ __global__ void __launch_bounds__(kAfThreads, kAfCtasPerSm) assignKernelF(KMeans
         tmemWaitTie(rh);
         tmemWaitTie(rl);
         tcFenceBefore(); // the next tile's MMA overwrites these columns after the barriers below
-        const uint32_t row = tid;
-        const bool valid = row < ti.count;
         float best = __int_as_float(0x7F800000), second = best;
         uint32_t bi = 0;
 #pragma unroll
@@ -348,8 +405,7 @@ __global__ void __launch_bounds__(kAfThreads, kAfCtasPerSm) assignKernelF(KMeans
             if (valid) L0.assign[uint64_t(ti.start) + row] = static_cast<uint8_t>(bi);
         } else {
             if (valid) {
-                const uint64_t at = uint64_t(ti.start) + row;
-                if (L0.assign[at] != bi) atomicAdd(&S.chg, 1u);
+                if (prevAssign != bi) atomicAdd(&S.chg, 1u);
                 L0.assign[at] = static_cast<uint8_t>(bi);
                 atomicAdd(&S.cnt[bi], 1u);
                 atomicAdd(&S.q[bi], (unsigned long long)S.xn[row]);
@@ -368,6 +424,10 @@ __global__ void __launch_bounds__(kAfThreads, kAfCtasPerSm) assignKernelF(KMeans
             }
         }
         __syncthreads(); // the tiles, bsel and xn are rewritten by the next step
+        t = n1;
+        ti = tn1;
+        n1 = n2;
+        tn1 = tn2;
     }
     flush();
     if (tid == 0) {
