@@ -52,8 +52,6 @@ constexpr uint32_t kPrepThreads = 512;
 constexpr uint32_t kScoreThreads = 1024;
 constexpr uint32_t kFlatList = 256;        // leaf lists shorter than this are walked flattened per warp batch
 constexpr uint32_t kFlatDepth = 8;         // pairs per lane in flight in the flattened walk
-constexpr uint32_t kLongMax = 384;         // long leaf lists queued per CTA for the shared walk
-constexpr uint32_t kLongChunk = 256;       // pairs per chunk of the shared walk (8 per lane)
 constexpr uint32_t kSegThreads = 256;
 constexpr uint32_t kSmemDocs = 20480;     // per-document accumulators kept in shared memory
 constexpr uint32_t kShardDocs = 2560;     // documents per inverted-file shard
@@ -671,11 +669,6 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
     __shared__ uint32_t nTouched;
     __shared__ uint32_t nextBatch; // entry batches are handed to warps as they finish
     __shared__ unsigned long long sel[kMaxK];
-    // Long leaf lists, walked after the batches in kLongChunk-pair chunks that any warp takes, so
-    // that a few long lists do not leave one warp working while the others wait
-    __shared__ uint32_t nLong, nextChunk;
-    __shared__ uint32_t longA[kLongMax][2], longLen0[kLongMax], longLen[kLongMax], longChunk[kLongMax + 1];
-    __shared__ float longQ[kLongMax];
     const uint32_t q = P.order ? P.order[blockIdx.x] : blockIdx.x;
     const uint32_t shard = blockIdx.y;
     const uint32_t docBeg = kSharded ? shard * P.shardDocs : 0u;
@@ -692,8 +685,6 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
     if (threadIdx.x == 0) {
         nTouched = 0;
         nextBatch = 0;
-        nLong = 0;
-        nextChunk = 0;
     }
     __syncthreads();
 
@@ -786,19 +777,7 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
         }
         const uint32_t len = (b0 - a0) + (b1 - a1);
         const bool flat = valid && leaf && len < kFlatList;
-        // long leaf lists go to the shared walk while it has room
-        const bool isLong = valid && leaf && !flat;
-        const uint32_t qslot = warpSlot(isLong, &nLong);
-        const bool queued = isLong && qslot < kLongMax;
-        if (queued) {
-            longA[qslot][0] = a0;
-            longA[qslot][1] = a1;
-            longLen0[qslot] = b0 - a0;
-            longLen[qslot] = len;
-            longChunk[qslot] = (len + kLongChunk - 1) / kLongChunk;
-            longQ[qslot] = qv;
-        }
-        for (uint32_t one = __ballot_sync(0xFFFFFFFFu, valid && !flat && !queued); one != 0; one &= one - 1) {
+        for (uint32_t one = __ballot_sync(0xFFFFFFFFu, valid && !flat); one != 0; one &= one - 1) {
             const uint32_t j = __ffs(one) - 1;
             const uint32_t ja0 = __shfl_sync(0xFFFFFFFFu, a0, j), jb0 = __shfl_sync(0xFFFFFFFFu, b0, j);
             const uint32_t ja1 = __shfl_sync(0xFFFFFFFFu, a1, j), jb1 = __shfl_sync(0xFFFFFFFFu, b1, j);
@@ -844,57 +823,6 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
 #pragma unroll
             for (uint32_t u = 0; u < kFlatDepth; u++)
                 if (f0 + 32u * u + lane < total) addPair(pr[u], pq[u]);
-        }
-    }
-    __syncthreads();
-    // The shared walk: chunk offsets of the queued lists (exclusive scan), then chunks on demand.
-    const uint32_t nl = min(nLong, kLongMax);
-    if (nl > 0) {
-        if (threadIdx.x < 32) {
-            uint32_t run = 0;
-            for (uint32_t i0 = 0; i0 < nl; i0 += 32) {
-                const uint32_t i = i0 + lane;
-                const uint32_t c = i < nl ? longChunk[i] : 0u;
-                uint32_t incl = c;
-#pragma unroll
-                for (uint32_t off = 1; off < 32; off <<= 1) {
-                    const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
-                    if (lane >= off) incl += v;
-                }
-                if (i < nl) longChunk[i] = run + incl - c;
-                run += __shfl_sync(0xFFFFFFFFu, incl, 31);
-            }
-            if (lane == 0) longChunk[nl] = run;
-        }
-        __syncthreads();
-        const uint32_t chunks = longChunk[nl];
-        for (;;) {
-            uint32_t c = 0;
-            if (lane == 0) c = atomicAdd(&nextChunk, 1u);
-            c = __shfl_sync(0xFFFFFFFFu, c, 0);
-            if (c >= chunks) break;
-            // the list holding chunk c: the last i with longChunk[i] <= c
-            uint32_t lo = 0, hi = nl;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (longChunk[mid] <= c) lo = mid;
-                else hi = mid;
-            }
-            const uint32_t first = (c - longChunk[lo]) * kLongChunk;
-            const uint32_t len0 = longLen0[lo], len = longLen[lo];
-            const uint32_t a0 = longA[lo][0], a1 = longA[lo][1];
-            const float qv = longQ[lo];
-            // pairs [first, first + kLongChunk) of the list: segment 0's range, then segment 1's
-            uint64_t pr[kLongChunk / 32];
-#pragma unroll
-            for (uint32_t u = 0; u < kLongChunk / 32; u++) {
-                const uint32_t t = first + 32u * u + lane;
-                pr[u] = 0;
-                if (t < len) pr[u] = t < len0 ? P.seg[0].pairs[a0 + t] : P.seg[1].pairs[a1 + (t - len0)];
-            }
-#pragma unroll
-            for (uint32_t u = 0; u < kLongChunk / 32; u++)
-                if (first + 32u * u + lane < len) addPair(pr[u], qv);
         }
     }
     __syncthreads();
