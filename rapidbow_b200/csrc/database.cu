@@ -545,13 +545,16 @@ struct ScoreParams {
 __device__ __forceinline__ float termOf(float q, float d) { return fabsf(q - d) - (q + d); }
 
 // Adds a term to a document of this CTA's shard (local index `i` < shard size).
-__device__ __forceinline__ void addTerm(unsigned long long* acc, uint8_t* touched, uint32_t i, float term)
+// Terms are -2 min(q, d) <= 0.  A term that rounds to 0 (|term| < 2^-57, e.g. a word whose idf
+// was clamped to FLT_MIN) is added as -1 unit instead, so that a document is touched exactly
+// when its accumulator is non-zero and no separate mark is stored per pair.  The change is at
+// most 2^-56 per term, far below the 2^-24 resolution of the float score near 2.
+__device__ __forceinline__ void addTerm(unsigned long long* acc, uint32_t i, float term)
 {
     // term * 2^56 is exact in fp32 (|term| <= 2, a power-of-two scale), so rounding it to the
     // nearest integer in fp32 gives the value llrint(double(term) * 2^56) would, without FP64
     const long long fx = __float2ll_rn(term * 0x1p56f);
-    atomicAdd(&acc[i], static_cast<unsigned long long>(fx));
-    touched[i] = 1; // every writer stores the same value
+    atomicAdd(&acc[i], static_cast<unsigned long long>(fx < 0 ? fx : -1ll));
 }
 
 // Float bits mapped so that unsigned order is numeric order (negative scores included).
@@ -677,11 +680,7 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
     // the shared-window form the compiler picks for a known shared-memory address.
     unsigned long long* acc;
     asm("mov.b64 %0, %1;" : "=l"(acc) : "l"(reinterpret_cast<unsigned long long*>(dyn)));
-    uint8_t* touched = reinterpret_cast<uint8_t*>(dyn + P.shardDocs);
-    for (uint32_t i = threadIdx.x; i < nLocal; i += blockDim.x) {
-        acc[i] = 0;
-        touched[i] = 0;
-    }
+    for (uint32_t i = threadIdx.x; i < nLocal; i += blockDim.x) acc[i] = 0;
     if (threadIdx.x == 0) {
         nTouched = 0;
         nextBatch = 0;
@@ -717,7 +716,7 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
     };
     auto addPair = [&](uint64_t pr, float qv) {
         const uint32_t i = static_cast<uint32_t>(pr >> 32) - docBeg;
-        if (!kSharded || i < nLocal) addTerm(acc, touched, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
+        if (!kSharded || i < nLocal) addTerm(acc, i, termOf(qv, __uint_as_float(static_cast<uint32_t>(pr))));
     };
     // A leaf word's list [a, b) by the whole warp, eight pairs per lane in flight.
     auto leafList = [&](const uint64_t* pairs, uint32_t a, uint32_t b, float qv) {
@@ -747,7 +746,7 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
             for (uint32_t r = p; r < b; r++)
                 if (static_cast<uint32_t>(pairs[r] >> 32) == slot) tf += P.seg[s].tf[r];
             const float d = float(tf) * w * P.rcpF[slot];
-            addTerm(acc, touched, slot - docBeg, termOf(qv, d));
+            addTerm(acc, slot - docBeg, termOf(qv, d));
         }
     };
     // Entries in batches of 32 per warp: lane j fetches entry base + j, its weight and its
@@ -832,7 +831,7 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 1024 / kThrea
     uint32_t myTouched = 0;
     for (uint32_t i = threadIdx.x; i < nLocal; i += blockDim.x) {
         unsigned long long key = ~0ull;
-        if (touched[i]) {
+        if (acc[i] != 0) { // touched: every term adds at least one unit
             const double sum = static_cast<double>(static_cast<long long>(acc[i])) / kFixScale;
             const float score = float(sum + 2.0f);
             key = (static_cast<unsigned long long>(orderedBits(score)) << 32) | P.slotDoc[docBeg + i];
@@ -925,7 +924,7 @@ struct Segment {
 // launch uses: changing a function's attribute between launches can wait for that function's
 // launches in flight on other streams.
 constexpr int kPrepSmemMax = int(kMaxDocDesc) * 4;
-constexpr int kScoreSmemMax = int(kSmemDocs) * 9;
+constexpr int kScoreSmemMax = int(kSmemDocs) * 8;
 
 template <uint32_t kThreads>
 void launchScore(bool sharded, dim3 grid, size_t smem, cudaStream_t stream, const ScoreParams& P)
@@ -1172,7 +1171,7 @@ public:
             P.outCount = dCount;
             // 1,024 threads per CTA whatever its document range: the pair walk is bound by load
             // latency, so a query split over few CTAs needs every warp an SM can hold
-            const size_t smem = size_t(shardDocs) * 9;
+            const size_t smem = size_t(shardDocs) * 8;
             launchScore<kScoreThreads>(shards > 1, dim3(nq, shards), smem, stream, P);
             if (shards > 1) {
                 ScopedKernelTimer mergeTimer(kTimedScoreMerge, stream);
