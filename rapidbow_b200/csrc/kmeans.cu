@@ -185,69 +185,30 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t& s)
     return z ^ (z >> 31);
 }
 
-__device__ __forceinline__ uint32_t dist128Dev(const uint8_t* a, const uint8_t* b)
-{
-    const uint4* a4 = reinterpret_cast<const uint4*>(a);
-    const uint4* b4 = reinterpret_cast<const uint4*>(b);
-    uint32_t acc = 0;
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const uint4 x = a4[k], y = b4[k];
-        const uint32_t d0 = __vabsdiffu4(x.x, y.x), d1 = __vabsdiffu4(x.y, y.y);
-        const uint32_t d2 = __vabsdiffu4(x.z, y.z), d3 = __vabsdiffu4(x.w, y.w);
-        acc = __dp4a(d0, d0, acc);
-        acc = __dp4a(d1, d1, acc);
-        acc = __dp4a(d2, d2, acc);
-        acc = __dp4a(d3, d3, acc);
-    }
-    return acc;
-}
-
 constexpr uint32_t kPPSample = 256;
+constexpr uint32_t kPPWarps = kPPSample / 32;
 
 // One CTA (256 threads) per node.  Same specification as the oracle's orc_kmeanspp_init:
 // SplitMix64 stream seeded by (seed, level, node); Floyd sampling of min(n, 256) member
 // positions (sorted); first center uniform; then D^2 sampling with exact integer weights.
+// Floyd's draws are sequential, so warp 0 runs them, checking each draw against the set so far
+// with all 32 lanes; the positions are then sorted by rank (they are distinct).  Thread i keeps
+// candidate i's row in registers and its D^2 weight; each pick's prefix sums are warp scans plus
+// one pass over the eight warp totals, and every thread draws the same random numbers, so a pick
+// costs two barriers.
 __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint64_t seed, uint32_t level,
                                                             uint32_t* nValidOut)
 {
     __shared__ uint32_t pos[kPPSample];
     __shared__ uint32_t cand[kPPSample];
-    __shared__ unsigned long long d2[kPPSample];
-    __shared__ unsigned long long pre[kPPSample];
+    __shared__ unsigned long long warpSum[kPPWarps];
+    __shared__ __align__(16) uint4 pickRow[kDims / 16];
     __shared__ uint32_t chosen[kMaxBranch];
-    __shared__ uint32_t nChosen;
-    __shared__ unsigned long long tPick;
     __shared__ uint64_t rngState;
     const uint32_t g = blockIdx.x;
     const uint32_t n = lv.nodeCnt[g];
-    const uint32_t tid = threadIdx.x;
+    const uint32_t tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
     const uint32_t S = n < kPPSample ? n : kPPSample;
-    if (tid == 0) {
-        uint64_t s = seed ^ (uint64_t(level) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(g) * 0xD1B54A32D192ED03ull);
-        if (n > kPPSample) {
-            uint32_t m = 0;
-            for (uint32_t j = n - S; j < n; j++) {
-                const uint32_t t = static_cast<uint32_t>(splitmix64(s) % (uint64_t(j) + 1));
-                bool found = false;
-                for (uint32_t q = 0; q < m; q++) found |= (pos[q] == t);
-                pos[m++] = found ? j : t;
-            }
-            // insertion sort (<= 256 entries)
-            for (uint32_t a = 1; a < m; a++) {
-                const uint32_t v = pos[a];
-                int32_t q = int32_t(a) - 1;
-                while (q >= 0 && pos[q] > v) {
-                    pos[q + 1] = pos[q];
-                    q--;
-                }
-                pos[q + 1] = v;
-            }
-        }
-        rngState = s;
-        nChosen = 0;
-    }
-    __syncthreads();
     if (n == 0) {
         if (tid == 0) nValidOut[g] = 0;
         for (uint32_t i = tid; i < kMaxBranch * 8; i += blockDim.x) {
@@ -256,52 +217,94 @@ __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint
         }
         return;
     }
-    if (tid < S) cand[tid] = lv.members[lv.nodeOff[g] + (n > kPPSample ? pos[tid] : tid)];
-    __syncthreads();
-    if (tid == 0) {
-        uint64_t s = rngState;
-        chosen[0] = static_cast<uint32_t>(splitmix64(s) % S);
-        rngState = s;
-        nChosen = 1;
-    }
-    __syncthreads();
-    if (tid < S) d2[tid] = dist128Dev(lv.desc + uint64_t(cand[tid]) * kDims, lv.desc + uint64_t(cand[chosen[0]]) * kDims);
-    __syncthreads();
-    for (uint32_t k = 1; k < lv.B; k++) {
-        // inclusive prefix of d2 (Hillis-Steele in shared memory)
-        if (tid < kPPSample) pre[tid] = tid < S ? d2[tid] : 0ull;
-        __syncthreads();
-        for (uint32_t off = 1; off < kPPSample; off <<= 1) {
-            unsigned long long v = 0;
-            if (tid >= off) v = pre[tid - off];
-            __syncthreads();
-            pre[tid] += v;
-            __syncthreads();
-        }
-        const unsigned long long total = pre[S - 1];
-        if (total == 0) break; // uniform across the CTA
-        if (tid == 0) {
-            uint64_t s = rngState;
-            tPick = splitmix64(s) % total;
-            rngState = s;
-        }
-        __syncthreads();
-        // smallest i with pre[i] > t
-        if (tid < S) {
-            const bool hit = pre[tid] > tPick && (tid == 0 || pre[tid - 1] <= tPick);
-            if (hit) {
-                chosen[k] = tid;
-                nChosen = k + 1;
+    uint64_t s = seed ^ (uint64_t(level) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(g) * 0xD1B54A32D192ED03ull);
+    if (n > kPPSample) {
+        if (warp == 0) {
+            for (uint32_t j = n - S, m = 0; j < n; j++, m++) {
+                const uint32_t t = static_cast<uint32_t>(splitmix64(s) % (uint64_t(j) + 1));
+                bool found = false;
+                for (uint32_t q = lane; q < m; q += 32) found |= (pos[q] == t);
+                found = __any_sync(0xFFFFFFFFu, found);
+                if (lane == 0) pos[m] = found ? j : t;
+                __syncwarp();
             }
+            if (lane == 0) rngState = s;
         }
         __syncthreads();
-        if (tid < S) {
-            const uint32_t d = dist128Dev(lv.desc + uint64_t(cand[tid]) * kDims, lv.desc + uint64_t(cand[chosen[k]]) * kDims);
-            if (d < d2[tid]) d2[tid] = d;
-        }
-        __syncthreads();
+        s = rngState;
+        // ascending order: the positions are distinct, so each one's rank is its slot
+        const uint32_t v = pos[tid];
+        uint32_t r = 0;
+        for (uint32_t q = 0; q < kPPSample; q++) r += pos[q] < v ? 1u : 0u;
+        cand[r] = lv.members[lv.nodeOff[g] + v];
+    } else if (tid < S) {
+        cand[tid] = lv.members[lv.nodeOff[g] + tid];
     }
-    const uint32_t nv = nChosen;
+    __syncthreads();
+    const bool mine = tid < S;
+    uint4 row[kDims / 16];
+#pragma unroll
+    for (uint32_t c = 0; c < kDims / 16; c++)
+        row[c] = mine ? reinterpret_cast<const uint4*>(lv.desc + uint64_t(cand[tid]) * kDims)[c] : make_uint4(0, 0, 0, 0);
+    // the squared distance of this thread's row to the picked row in shared memory
+    auto distToPick = [&]() -> unsigned long long {
+        uint32_t acc = 0;
+#pragma unroll
+        for (uint32_t c = 0; c < kDims / 16; c++) {
+            const uint4 y = pickRow[c];
+            const uint32_t d0 = __vabsdiffu4(row[c].x, y.x), d1 = __vabsdiffu4(row[c].y, y.y);
+            const uint32_t d2v = __vabsdiffu4(row[c].z, y.z), d3 = __vabsdiffu4(row[c].w, y.w);
+            acc = __dp4a(d0, d0, acc);
+            acc = __dp4a(d1, d1, acc);
+            acc = __dp4a(d2v, d2v, acc);
+            acc = __dp4a(d3, d3, acc);
+        }
+        return acc;
+    };
+    uint32_t pick = static_cast<uint32_t>(splitmix64(s) % S);
+    if (tid == 0) chosen[0] = pick;
+    if (tid == pick) {
+#pragma unroll
+        for (uint32_t c = 0; c < kDims / 16; c++) pickRow[c] = row[c];
+    }
+    __syncthreads();
+    unsigned long long d2 = mine ? distToPick() : 0ull;
+    uint32_t nv = 1;
+    for (uint32_t k = 1; k < lv.B; k++) {
+        // inclusive prefix of d2 over the candidates: warp scan, then the earlier warps' totals
+        unsigned long long incl = d2;
+#pragma unroll
+        for (uint32_t off = 1; off < 32; off <<= 1) {
+            const unsigned long long v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+            if (lane >= off) incl += v;
+        }
+        if (lane == 31) warpSum[warp] = incl;
+        __syncthreads();
+        unsigned long long before = 0, total = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < kPPWarps; w++) {
+            const unsigned long long v = warpSum[w];
+            before += w < warp ? v : 0ull;
+            total += v;
+        }
+        if (total == 0) break; // uniform across the CTA
+        incl += before;
+        const unsigned long long t = splitmix64(s) % total;
+        // smallest i with prefix[i] > t: exactly one candidate has prefix > t >= prefix - d2
+        const bool hit = mine && incl > t && incl - d2 <= t;
+        if (hit) {
+            chosen[k] = tid;
+#pragma unroll
+            for (uint32_t c = 0; c < kDims / 16; c++) pickRow[c] = row[c];
+        }
+        nv = k + 1;
+        __syncthreads();
+        if (mine) {
+            const unsigned long long d = distToPick();
+            if (d < d2) d2 = d;
+        }
+        __syncthreads(); // pickRow and warpSum are rewritten by the next pick
+    }
     if (tid == 0) nValidOut[g] = nv;
     for (uint32_t i = tid; i < kMaxBranch * 8; i += blockDim.x) {
         const uint32_t b = i / 8, chunk = i % 8;

@@ -41,6 +41,18 @@ def test_build_kmeanspp_matches_oracle(oracle, B, L, n, iters):
     _tree_equal(voc, ref)
 
 
+@pytest.mark.parametrize("n_distinct,n", [(6, 3000), (40, 600), (300, 5000)])
+def test_build_kmeanspp_duplicates_match_oracle(oracle, n_distinct, n):
+    """Few distinct rows: the D^2 weights reach zero before B picks (fewer valid centers, empty
+    children at the next level) and the sampled candidates repeat."""
+    base = sift_like(n_distinct, seed=321 + n_distinct).numpy()
+    desc = np.ascontiguousarray(base[np.random.default_rng(n).integers(0, n_distinct, n)])
+    voc = rbw.build_vocabulary(torch.from_numpy(desc).cuda(), 16, nb_doc=20, nb_levels=2, init="kmeans++", seed=99,
+                               max_iterations=10, ieee_division=True)
+    ref = oracle.build_vocabulary(desc, 20, 16, 2, max_iter=10, init=INIT_KMEANSPP, seed=99)
+    _tree_equal(voc, ref)
+
+
 def test_build_matches_reference_build(reference):
     """Bit-identical blob with the reference's own buildVocabulary (same default-seeded RNG)."""
     desc = sift_like(30000, seed=77).numpy()
