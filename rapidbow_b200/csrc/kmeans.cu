@@ -175,14 +175,20 @@ __global__ void centerNormsKernel(KMeansLevel lv)
 }
 
 // ------------------------------------------------------------------ k-means++ init
-__device__ __forceinline__ uint64_t splitmix64(uint64_t& s)
+// SplitMix64 (Steele, Lea, Flood 2014): the output for state z; the generator adds
+// kSplitMixGamma to the state before each output, so draw i (from 0) of a stream started at s
+// is splitMixOut(s + (i + 1) * kSplitMixGamma).
+constexpr uint64_t kSplitMixGamma = 0x9E3779B97F4A7C15ull;
+__device__ __forceinline__ uint64_t splitMixOut(uint64_t z)
 {
-    // SplitMix64 (Steele, Lea, Flood 2014).
-    s += 0x9E3779B97F4A7C15ull;
-    uint64_t z = s;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
+}
+__device__ __forceinline__ uint64_t splitmix64(uint64_t& s)
+{
+    s += kSplitMixGamma;
+    return splitMixOut(s);
 }
 
 constexpr uint32_t kPPSample = 256;
@@ -191,20 +197,30 @@ constexpr uint32_t kPPWarps = kPPSample / 32;
 // One CTA (256 threads) per node.  Same specification as the oracle's orc_kmeanspp_init:
 // SplitMix64 stream seeded by (seed, level, node); Floyd sampling of min(n, 256) member
 // positions (sorted); first center uniform; then D^2 sampling with exact integer weights.
-// Floyd's draws are sequential, so warp 0 runs them, checking each draw against the set so far
-// with all 32 lanes; the positions are then sorted by rank (they are distinct).  Thread i keeps
-// candidate i's row in registers and its D^2 weight; each pick's prefix sums are warp scans plus
-// one pass over the eight warp totals, and every thread draws the same random numbers, so a pick
-// costs two barriers.
+// Floyd's draws do not depend on the set, so thread m makes draw m, t_m = out_m % (j_m + 1) with
+// j_m = n - 256 + m, directly from the counter-based stream.  Step m inserts j_m when t_m is
+// already in the set, else t_m; with base = n - 256:
+//   - t_m < base: t_m is in the set iff an earlier draw equals it (values below base enter only
+//     as themselves, and the first equal draw did enter);
+//   - t_m = base + m: not yet in the set (every earlier value is below j_m);
+//   - t_m = j_r, r < m: in the set iff step r inserted j_r (found_r) or a draw t_q, r <= q < m,
+//     equals it;
+// so found_m = local_m || found_r along links m -> r < m, an OR over a chain of at most 256
+// steps, resolved by eight rounds of pointer jumping.  The distinct positions are then sorted by
+// rank (each thread counts the smaller ones).  Thread i keeps candidate i's row in registers and
+// its D^2 weight; each pick's prefix sums are warp scans plus one pass over the eight warp totals,
+// and every thread draws the same random numbers, so a pick costs two barriers.
 __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint64_t seed, uint32_t level,
                                                             uint32_t* nValidOut)
 {
     __shared__ uint32_t pos[kPPSample];
     __shared__ uint32_t cand[kPPSample];
+    __shared__ uint32_t draw[kPPSample];
+    __shared__ uint32_t link[kPPSample];
+    __shared__ uint8_t found[kPPSample];
     __shared__ unsigned long long warpSum[kPPWarps];
     __shared__ __align__(16) uint4 pickRow[kDims / 16];
     __shared__ uint32_t chosen[kMaxBranch];
-    __shared__ uint64_t rngState;
     const uint32_t g = blockIdx.x;
     const uint32_t n = lv.nodeCnt[g];
     const uint32_t tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
@@ -219,24 +235,46 @@ __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint
     }
     uint64_t s = seed ^ (uint64_t(level) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(g) * 0xD1B54A32D192ED03ull);
     if (n > kPPSample) {
-        if (warp == 0) {
-            for (uint32_t j = n - S, m = 0; j < n; j++, m++) {
-                const uint32_t t = static_cast<uint32_t>(splitmix64(s) % (uint64_t(j) + 1));
-                bool found = false;
-                for (uint32_t q = lane; q < m; q += 32) found |= (pos[q] == t);
-                found = __any_sync(0xFFFFFFFFu, found);
-                if (lane == 0) pos[m] = found ? j : t;
-                __syncwarp();
-            }
-            if (lane == 0) rngState = s;
-        }
+        constexpr uint32_t kNone = 0xFFFFFFFFu;
+        const uint32_t base = n - kPPSample;
+        const uint32_t t = static_cast<uint32_t>(splitMixOut(s + uint64_t(tid + 1) * kSplitMixGamma) %
+                                                 (uint64_t(base) + tid + 1));
+        draw[tid] = t;
         __syncthreads();
-        s = rngState;
+        bool f = false;
+        uint32_t lk = kNone, q0 = 0;
+        if (t >= base) {
+            const uint32_t r = t - base;
+            q0 = r < tid ? r : tid; // r == tid: nothing to compare, no link
+            if (r < tid) lk = r;
+        }
+        for (uint32_t q = q0; q < tid; q++) f |= draw[q] == t;
+        found[tid] = f ? 1 : 0;
+        link[tid] = lk;
+        __syncthreads();
+#pragma unroll 1
+        for (uint32_t round = 0; round < 8; round++) {
+            bool nf = f;
+            uint32_t nl = lk;
+            if (lk != kNone) {
+                nf = f || found[lk] != 0;
+                nl = link[lk];
+            }
+            __syncthreads();
+            f = nf;
+            lk = nl;
+            found[tid] = f ? 1 : 0;
+            link[tid] = lk;
+            __syncthreads();
+        }
+        pos[tid] = f ? base + tid : t;
+        s += uint64_t(kPPSample) * kSplitMixGamma; // the stream after the 256 draws
+        __syncthreads();
         // ascending order: the positions are distinct, so each one's rank is its slot
         const uint32_t v = pos[tid];
-        uint32_t r = 0;
-        for (uint32_t q = 0; q < kPPSample; q++) r += pos[q] < v ? 1u : 0u;
-        cand[r] = lv.members[lv.nodeOff[g] + v];
+        uint32_t rk = 0;
+        for (uint32_t q = 0; q < kPPSample; q++) rk += pos[q] < v ? 1u : 0u;
+        cand[rk] = lv.members[lv.nodeOff[g] + v];
     } else if (tid < S) {
         cand[tid] = lv.members[lv.nodeOff[g] + tid];
     }
