@@ -13,6 +13,7 @@
 #include <cstring>
 #include <limits>
 #include <numeric>
+#include <thread>
 #include <mutex>
 #include <random>
 #include <unordered_set>
@@ -482,7 +483,8 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
     RBW_CUDA(cudaMemsetAsync(sums.get(), 0, sums.bytes(), stream));
     RBW_CUDA(cudaMemsetAsync(changed.get(), 0, changed.bytes(), stream));
 
-    std::vector<uint32_t> occ(voc->mNbNodes * B, 0u);
+    // per-node occurrence counts stay on the device until the end (no host copy per level)
+    StreamBuffer occDev(voc->mNbNodes * B * 4, st);
     voc->mMasks.assign(voc->mNbNodes, 0u);
     std::mt19937_64 rng{}; // kmeans.cpp:145 (default seed)
     std::vector<uint32_t> hostCnt, hostPicks, hostNValid;
@@ -585,6 +587,9 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
             }
             iters = it + 1;
             if ((it + 1) % check == 0 || it + 1 == opts.maxIterations) {
+                // the host-side weight array is touched (its pages faulted in) while the device
+                // runs the level's first Lloyd steps, not after the last level
+                if (voc->mWeights.empty()) voc->mWeights.assign(voc->mNbNodes * B, 0.0f);
                 uint32_t active = 0;
                 RBW_CUDA(cudaMemcpyAsync(&active, activeCount, 4, cudaMemcpyDeviceToHost, stream));
                 RBW_CUDA(cudaStreamSynchronize(stream));
@@ -602,22 +607,45 @@ std::unique_ptr<Vocabulary> Vocabulary::build(uint32_t B, uint32_t L, const uint
         RegroupScratch rs{tileHist.as<uint32_t>(), tileScan.as<uint32_t>(), scanTmp.as<uint32_t>(),
                           tiles32.as<NodeTile>(), tileOff.as<uint32_t>(), totals, maxTiles32};
         launchRegroup(lv, rs, members2.as<uint32_t>(), childCnt.as<uint32_t>(), childOff.as<uint32_t>(), stream);
-        RBW_CUDA(cudaMemcpyAsync(occ.data() + lb * B, childCnt.get(), uint64_t(nbLv) * B * 4, cudaMemcpyDeviceToHost,
-                                 stream));
+        RBW_CUDA(cudaMemcpyAsync(occDev.as<uint32_t>() + lb * B, childCnt.get(), uint64_t(nbLv) * B * 4,
+                                 cudaMemcpyDeviceToDevice, stream));
         std::swap(members, members2);
         std::swap(nodeCnt, childCnt);
         std::swap(nodeOff, childOff);
     }
+    // the device finishes the tree while the host computes the idf weights
+    if (fl) voc->roundFloatCenters(stream);
+    voc->finalizeDevice(stream);
     if (fl) {
         RBW_CUDA(cudaMemcpyAsync(hostCounters.data(), counters.get(), hostCounters.size() * 8, cudaMemcpyDeviceToHost,
                                  stream));
     }
-    RBW_CUDA(cudaStreamSynchronize(stream));
+    // The counts land in the weights' own storage (one host buffer instead of two) and are
+    // turned into weights in place.  Many nodes share a count: the weights of counts below
+    // kIdfMemo are computed once (the same expression, so the same float).
+    static_assert(sizeof(float) == sizeof(uint32_t), "counts are staged in the weights array");
     voc->mWeights.resize(voc->mNbNodes * B);
-    for (size_t i = 0; i < occ.size(); i++) voc->mWeights[i] = idfWeight(nbDoc, occ[i]);
-    if (fl) voc->roundFloatCenters(stream);
-    voc->finalizeDevice(stream);
+    float* w = voc->mWeights.data();
+    const size_t nw = voc->mWeights.size();
+    RBW_CUDA(cudaMemcpyAsync(w, occDev.get(), nw * 4, cudaMemcpyDeviceToHost, stream));
+    // the weights of every count below kIdfMemo, computed once (the same expression, so the same
+    // float), while the copy runs
+    constexpr uint32_t kIdfMemo = 1u << 12;
+    float memo[kIdfMemo];
+    for (uint32_t c = 0; c < kIdfMemo; c++) memo[c] = idfWeight(nbDoc, c);
     RBW_CUDA(cudaStreamSynchronize(stream));
+    auto weigh = [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; i++) {
+            uint32_t c;
+            std::memcpy(&c, w + i, 4);
+            w[i] = c < kIdfMemo ? memo[c] : idfWeight(nbDoc, c);
+        }
+    };
+    const size_t nThreads = nw >= (size_t(1) << 18) ? 4 : 1;
+    std::vector<std::thread> helpers;
+    for (size_t k = 1; k < nThreads; k++) helpers.emplace_back(weigh, nw * k / nThreads, nw * (k + 1) / nThreads);
+    weigh(0, nw / nThreads);
+    for (auto& h : helpers) h.join();
     const DeviceErrors e = voc->takeDeviceErrors();
     if (e.code != 0)
         throw Error(kTimeout, "a bounded device wait gave up during the build (site " + std::to_string(e.where) + ")");
