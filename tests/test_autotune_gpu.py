@@ -77,6 +77,23 @@ def test_tensor_core_sums_give_the_oracle_build(oracle):
         assert np.array_equal(w, ref["weights"]), ctas
 
 
+@pytest.mark.parametrize("B,L,n,nb_doc", [(16, 3, 30000, 123), (10, 4, 60000, 50)])
+def test_tensor_core_sums_give_the_reference_build(reference, B, L, n, nb_doc):
+    """The tensor-core sums with the reference's fast-math center division: the B = 16 blob
+    equals the reference's own build, and with B = 10 (no reference build) the tree equals the
+    build with shared-atomic sums."""
+    desc_t = sift_like(n, seed=77 + B, device="cuda")
+    desc = desc_t.cpu().numpy()
+    at.set_value("assign_sums", B, 0, at.bucket(n), 2)
+    voc = rbw.build_vocabulary(desc_t, B, nb_doc=nb_doc, nb_levels=L, max_iterations=1000)
+    if B == 16:
+        assert voc.serialize() == reference.build_vocabulary(desc, nb_doc=nb_doc, L=L)
+    at.set_value("assign_sums", B, 0, at.bucket(n), 1)
+    base = rbw.build_vocabulary(desc_t, B, nb_doc=nb_doc, nb_levels=L, max_iterations=1000)
+    for a, b in zip(voc.tree(), base.tree()):
+        assert np.array_equal(a, b)
+
+
 def test_tuning_records_the_fastest_and_applies_it(tmp_path):
     t = at.Autotuner.for_current_device(str(tmp_path / "tune.json"))
     B, L = 16, 4
