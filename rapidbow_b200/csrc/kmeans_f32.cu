@@ -459,6 +459,9 @@ __global__ void __launch_bounds__(256) updateKernelF(KMeansLevelF lv)
     }
     if (t < kMaxBranch) cnt[t] = L0.counts[uint64_t(g) * kMaxBranch + t];
     __syncthreads();
+    // A node frozen before this step was skipped by the assign (ch is 0 then): nothing was
+    // accumulated, every counter is zero and its inertia is that of its last assignment.
+    if (!ran) return;
     float* c = lv.centers + uint64_t(g) * kMaxBranch * kDims;
     unsigned long long* sums = L0.sums + uint64_t(g) * kMaxBranch * kDims;
     unsigned long long* q = lv.q + uint64_t(g) * kMaxBranch;
@@ -494,9 +497,9 @@ __global__ void __launch_bounds__(256) updateKernelF(KMeansLevelF lv)
             if (b < B && cnt[b] != 0) c[i] = __double2float_rn(__ddiv_rn(double(sums[i]), double(cnt[b])));
         }
     }
-    for (uint32_t i = t; i < kMaxBranch * kDims; i += blockDim.x) sums[i] = 0ull;
+    for (uint32_t i = t; i < B * kDims; i += blockDim.x) sums[i] = 0ull; // centers b >= B have none
     __syncthreads();
-    if (t < kMaxBranch) {
+    if (t < B) {
         L0.counts[uint64_t(g) * kMaxBranch + t] = 0;
         q[t] = 0ull;
     }
