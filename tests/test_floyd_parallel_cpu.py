@@ -1,5 +1,6 @@
-"""The k-means++ kernel makes Floyd's sampling draws in parallel (rapidbow_b200/csrc/kmeans.cu, kmeansPPKernel):
-thread m draws t_m = out_m mod (j_m + 1) from the counter-based SplitMix64 stream, and whether
+"""The k-means++ kernel (kmeansPPKernel in rapidbow_b200/csrc/kmeans.cu) makes Floyd's sampling
+draws in parallel: thread m draws t_m = out_m mod (j_m + 1) from the counter-based SplitMix64
+stream, and whether
 step m inserts j_m (t_m already taken) follows from the draws alone, except for t_m = j_r with
 r < m, where it also depends on step r: found_m = local_m or found_r, resolved by eight rounds of
 pointer jumping.  This restates that formulation in Python and checks it against the sequential
