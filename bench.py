@@ -38,10 +38,10 @@ BYTES_PER_DESC = 132  # 128 B read + 4 B leaf written (algorithmic, per descript
 # of an ncu capture of a 2M-descriptor lookup (B=16, L=4; both pass launches averaged).  Traffic
 # grows in proportion to the descriptors, so it is scaled to the timed launch.
 LOOKUP_PASS_DRAM_BYTES_PER_DESC = 136.6
-# DRAM bytes of one scoring launch (queryPrepKernel + scoreKernel: 2.6 MB + 1.383 GB read,
-# 4.1 MB written) on the seeded 20,000-image database with 256 queries, top-50, from an ncu
+# DRAM bytes of one scoring launch (queryPrepKernel + scoreKernel: 2.6 MB + 1.388 GB read,
+# 3.9 MB written) on the seeded 20,000-image database with 256 queries, top-50, from an ncu
 # capture of that workload.
-SCORE_DRAM_BYTES_20K_IMAGES = 1_390_150_000
+SCORE_DRAM_BYTES_20K_IMAGES = 1_394_930_000
 WORKLOAD = ("lookup of 10M fresh SIFT-like descriptors per GPU through a 65,536-word tree "
             "(B=16, L=4) trained on 2M descriptors (k-means++ init, 10 Lloyd iterations)")
 
