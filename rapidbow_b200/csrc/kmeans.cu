@@ -193,6 +193,7 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t& s)
 
 constexpr uint32_t kPPSample = 256;
 constexpr uint32_t kPPWarps = kPPSample / 32;
+constexpr uint32_t kPPCtasPerSm = 6; // by shared memory: 32 KB of candidate rows per CTA
 
 // One CTA (256 threads) per node.  Same specification as the oracle's orc_kmeanspp_init:
 // SplitMix64 stream seeded by (seed, level, node); Floyd sampling of min(n, 256) member
@@ -207,19 +208,22 @@ constexpr uint32_t kPPWarps = kPPSample / 32;
 //     equals it;
 // so found_m = local_m || found_r along links m -> r < m, an OR over a chain of at most 256
 // steps, resolved by eight rounds of pointer jumping.  The distinct positions are then sorted by
-// rank (each thread counts the smaller ones).  Thread i keeps candidate i's row in registers and
-// its D^2 weight; each pick's prefix sums are warp scans plus one pass over the eight warp totals,
-// and every thread draws the same random numbers, so a pick costs two barriers.
-__global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint64_t seed, uint32_t level,
-                                                            uint32_t* nValidOut)
+// rank (each thread counts the smaller ones).  The candidate rows sit in shared memory and thread
+// i holds candidate i's D^2 weight; each pick's prefix sums are warp scans plus one pass over the
+// eight warp totals, and every thread draws the same random numbers, so a pick costs two
+// barriers.  Registers stay low enough for six CTAs per SM (deep levels have 10^5 nodes).
+__global__ void __launch_bounds__(kPPSample, kPPCtasPerSm) kmeansPPKernel(KMeansLevel lv, uint64_t seed,
+                                                                          uint32_t level, uint32_t* nValidOut)
 {
+    // candidate rows, chunk c of row i at [i][c ^ (i & 7)] (a quarter-warp reading its own rows
+    // hits 32 different banks)
+    __shared__ uint4 rowS[kPPSample][kDims / 16];
     __shared__ uint32_t pos[kPPSample];
     __shared__ uint32_t cand[kPPSample];
     __shared__ uint32_t draw[kPPSample];
     __shared__ uint32_t link[kPPSample];
     __shared__ uint8_t found[kPPSample];
     __shared__ unsigned long long warpSum[kPPWarps];
-    __shared__ __align__(16) uint4 pickRow[kDims / 16];
     __shared__ uint32_t chosen[kMaxBranch];
     const uint32_t g = blockIdx.x;
     const uint32_t n = lv.nodeCnt[g];
@@ -280,18 +284,20 @@ __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint
     }
     __syncthreads();
     const bool mine = tid < S;
-    uint4 row[kDims / 16];
+    // eight threads per row, 32 rows per round
 #pragma unroll
-    for (uint32_t c = 0; c < kDims / 16; c++)
-        row[c] = mine ? reinterpret_cast<const uint4*>(lv.desc + uint64_t(cand[tid]) * kDims)[c] : make_uint4(0, 0, 0, 0);
-    // the squared distance of this thread's row to the picked row in shared memory
-    auto distToPick = [&]() -> unsigned long long {
+    for (uint32_t k = 0; k < kPPSample / 32; k++) {
+        const uint32_t r = 32u * k + tid / 8, c = tid % 8;
+        if (r < S) rowS[r][c ^ (r & 7u)] = reinterpret_cast<const uint4*>(lv.desc + uint64_t(cand[r]) * kDims)[c];
+    }
+    // the squared distance of this thread's row to row p
+    auto distTo = [&](uint32_t p) -> unsigned long long {
         uint32_t acc = 0;
 #pragma unroll
         for (uint32_t c = 0; c < kDims / 16; c++) {
-            const uint4 y = pickRow[c];
-            const uint32_t d0 = __vabsdiffu4(row[c].x, y.x), d1 = __vabsdiffu4(row[c].y, y.y);
-            const uint32_t d2v = __vabsdiffu4(row[c].z, y.z), d3 = __vabsdiffu4(row[c].w, y.w);
+            const uint4 x = rowS[tid][c ^ (tid & 7u)], y = rowS[p][c ^ (p & 7u)];
+            const uint32_t d0 = __vabsdiffu4(x.x, y.x), d1 = __vabsdiffu4(x.y, y.y);
+            const uint32_t d2v = __vabsdiffu4(x.z, y.z), d3 = __vabsdiffu4(x.w, y.w);
             acc = __dp4a(d0, d0, acc);
             acc = __dp4a(d1, d1, acc);
             acc = __dp4a(d2v, d2v, acc);
@@ -299,14 +305,10 @@ __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint
         }
         return acc;
     };
-    uint32_t pick = static_cast<uint32_t>(splitmix64(s) % S);
+    const uint32_t pick = static_cast<uint32_t>(splitmix64(s) % S);
     if (tid == 0) chosen[0] = pick;
-    if (tid == pick) {
-#pragma unroll
-        for (uint32_t c = 0; c < kDims / 16; c++) pickRow[c] = row[c];
-    }
     __syncthreads();
-    unsigned long long d2 = mine ? distToPick() : 0ull;
+    unsigned long long d2 = mine ? distTo(pick) : 0ull;
     uint32_t nv = 1;
     for (uint32_t k = 1; k < lv.B; k++) {
         // inclusive prefix of d2 over the candidates: warp scan, then the earlier warps' totals
@@ -330,18 +332,14 @@ __global__ void __launch_bounds__(kPPSample) kmeansPPKernel(KMeansLevel lv, uint
         const unsigned long long t = splitmix64(s) % total;
         // smallest i with prefix[i] > t: exactly one candidate has prefix > t >= prefix - d2
         const bool hit = mine && incl > t && incl - d2 <= t;
-        if (hit) {
-            chosen[k] = tid;
-#pragma unroll
-            for (uint32_t c = 0; c < kDims / 16; c++) pickRow[c] = row[c];
-        }
+        if (hit) chosen[k] = tid;
         nv = k + 1;
         __syncthreads();
         if (mine) {
-            const unsigned long long d = distToPick();
+            const unsigned long long d = distTo(chosen[k]);
             if (d < d2) d2 = d;
         }
-        __syncthreads(); // pickRow and warpSum are rewritten by the next pick
+        __syncthreads(); // warpSum is rewritten by the next pick
     }
     if (tid == 0) nValidOut[g] = nv;
     for (uint32_t i = tid; i < kMaxBranch * 8; i += blockDim.x) {
