@@ -141,6 +141,38 @@ def test_norms_bit_exact_for_every_weight_spread(oracle, kind):
         check_query(db, odb, q, 25)
 
 
+def test_documents_touched_only_through_clamped_words_are_results(oracle):
+    """A document that shares with the query only words whose idf is clamped to FLT_MIN gets
+    terms that round to zero in the fixed-point sum; it is still a result (score 2), as in the
+    reference, when fewer than k documents are touched."""
+    B, L = 10, 3
+    centers, masks, weights = random_tree(B, L, 71, dup_rate=0.0)
+    fmin = np.float32(np.finfo(np.float32).tiny)
+    weights = np.full(weights.shape, 2.0, dtype=np.float32)
+    weights[:1 + B] = fmin                  # every upper-level word
+    n_leaves = B ** L
+    clamped = np.arange(0, 40, dtype=np.uint32)
+    weights[(1 + B) + clamped // B, clamped % B] = fmin
+    voc = rbw.vocabulary_from_host(B, L, centers, masks, weights)
+    db = rbw.DataBase(voc)
+    odb = oracle.db(B, L, weights)
+    docs = [
+        np.array([3, 7, 7, 12], dtype=np.uint32),          # clamped words only
+        np.array([5, 39, 500, 501], dtype=np.uint32),      # clamped words and others
+        np.array([520, 530, 999], dtype=np.uint32),        # a normal word shared with the query
+        np.array([700, 701, 702], dtype=np.uint32),        # upper-level words only in common
+        np.array([3], dtype=np.uint32),                     # one clamped word
+    ]
+    for i, d in enumerate(docs):
+        db.add_doc(i, d)
+        odb.add(i, d)
+    for q in (np.array([3, 7, 12, 530], dtype=np.uint32), np.array([3, 5], dtype=np.uint32),
+              np.array([7, 7, 7], dtype=np.uint32)):
+        got, scores = check_query(db, odb, q, 10)
+        odocs, _ = odb.query(q, 10, mode=0)
+        assert sorted(got.tolist()) == sorted(odocs.tolist())
+
+
 def test_self_query_ranks_itself_first(oracle):
     B, L = 16, 3
     docs = make_docs(200, B ** L, seed=3)
