@@ -9,7 +9,7 @@
 
 namespace rbw {
 
-// Owning device buffer, from the library's memory pool of the device current at allocation.
+// Owning device buffer.
 class DeviceBuffer
 {
 public:
@@ -17,7 +17,7 @@ public:
     explicit DeviceBuffer(size_t bytes) { reset(bytes); }
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    DeviceBuffer(DeviceBuffer&& o) noexcept : mPtr{o.mPtr}, mBytes{o.mBytes}, mDevice{o.mDevice}
+    DeviceBuffer(DeviceBuffer&& o) noexcept : mPtr{o.mPtr}, mBytes{o.mBytes}
     {
         o.mPtr = nullptr;
         o.mBytes = 0;
@@ -26,7 +26,6 @@ public:
     {
         std::swap(mPtr, o.mPtr);
         std::swap(mBytes, o.mBytes);
-        std::swap(mDevice, o.mDevice);
         return *this;
     }
     ~DeviceBuffer();
@@ -37,10 +36,8 @@ public:
     size_t bytes() const { return mBytes; }
 
 private:
-    void release();
     void* mPtr = nullptr;
     size_t mBytes = 0;
-    int mDevice = 0;
 };
 
 enum InitMode : uint32_t { kInitReference = 0, kInitKMeansPP = 1, kInitInjected = 2 };
